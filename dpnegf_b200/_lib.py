@@ -1,0 +1,117 @@
+"""ctypes binding of ``libnegf_b200.so`` (C ABI declared in include/negf_b200.h).
+
+The shared library is built in-tree by ``dpnegf_b200/csrc/build.py`` (also run
+by ``__graft_entry__.build()``).  There is no fallback: if the library is
+missing or no CUDA device is present, every entry point raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libnegf_b200.so")
+
+# status codes (include/negf_b200.h)
+NEGF_OK = 0
+NEGF_WARN_LS_CONVERGENCE = 1
+NEGF_ERR_LS_NOT_CONVERGED = 2
+NEGF_ERR_LS_RESIDUAL = 3
+NEGF_ERR_SINGULAR = 4
+NEGF_ERR_NONFINITE = 5
+NEGF_ERR_ARGUMENT = -1
+NEGF_ERR_UNSUPPORTED = -2
+NEGF_ERR_CUDA = -3
+NEGF_MAX_BLOCK = 512
+
+# RGF flags
+OUT_GTRANS = 1 << 0
+OUT_GR_LC = 1 << 1
+OUT_GRD = 1 << 2
+OUT_GRL = 1 << 3
+OUT_GRU = 1 << 4
+OUT_GR_LEFT = 1 << 5
+TRANS = 1 << 6
+ORB_DOS = 1 << 7
+LESSER = 1 << 8
+
+# numpy mirrors of the descriptor structs (packed exactly like the C structs)
+BLOCK_FIELDS = ["hd", "sd", "hu", "su", "hl", "sl", "orb0", "g", "o_grd", "o_grl", "o_gru", "o_grlc",
+                "o_grleft", "o_gnd", "o_gnl", "o_gnu", "o_ginleft", "s_in"]
+BLOCK_DTYPE = np.dtype([("n", "<i4"), ("n_next", "<i4")] + [(f, "<i8") for f in BLOCK_FIELDS])
+DEVICE_DTYPE = np.dtype([("n_blocks", "<i4"), ("blk0", "<i4"), ("n_orb", "<i4"), ("pad", "<i4"),
+                         ("o_gtrans", "<i8"), ("g_slab", "<i8")])
+ITEM_DTYPE = np.dtype([("dev", "<i4"), ("row", "<i4"), ("z_re", "<f8"), ("z_im", "<f8"),
+                       ("se_l", "<i8"), ("se_r", "<i8"), ("nse_l", "<i4"), ("nse_r", "<i4"),
+                       ("out", "<i8"), ("orb", "<i8")])
+
+
+class NegfRgfProblem(ctypes.Structure):
+    _fields_ = [
+        ("blocks", ctypes.c_void_p),
+        ("devices", ctypes.c_void_p),
+        ("items", ctypes.c_void_p),
+        ("n_items", ctypes.c_int32),
+        ("max_n", ctypes.c_int32),
+        ("max_g_slab", ctypes.c_int64),
+        ("hs", ctypes.c_void_p),
+        ("se", ctypes.c_void_p),
+        ("s_in", ctypes.c_void_p),
+        ("out", ctypes.c_void_p),
+        ("trans", ctypes.c_void_p),
+        ("orb_dos", ctypes.c_void_p),
+        ("status", ctypes.c_void_p),
+        ("flags", ctypes.c_uint32),
+        ("n_slots", ctypes.c_int32),
+        ("scratch", ctypes.c_void_p),
+        ("scratch_bytes", ctypes.c_size_t),
+    ]
+
+
+_lib = None
+
+
+class NegfError(RuntimeError):
+    pass
+
+
+def load():
+    """Load the CUDA library once; raise loudly when it is unavailable."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.isfile(LIB_PATH):
+        raise NegfError(f"{LIB_PATH} is missing: build it with `python dpnegf_b200/csrc/build.py` "
+                        "(dpnegf_b200 has no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    lib.negf_rgf_scratch_bytes.restype = ctypes.c_size_t
+    lib.negf_rgf_scratch_bytes.argtypes = [ctypes.POINTER(NegfRgfProblem)]
+    lib.negf_rgf_run.restype = ctypes.c_int
+    lib.negf_rgf_run.argtypes = [ctypes.POINTER(NegfRgfProblem), ctypes.c_void_p]
+    lib.negf_sm_count.restype = ctypes.c_int
+    lib.negf_sm_count.argtypes = []
+    lib.negf_version.restype = ctypes.c_char_p
+    lib.negf_abi_struct_size.restype = ctypes.c_size_t
+    lib.negf_abi_struct_size.argtypes = [ctypes.c_int]
+    _lib = lib
+    return lib
+
+
+def check(code, what):
+    if code != NEGF_OK:
+        names = {NEGF_ERR_ARGUMENT: "invalid argument", NEGF_ERR_UNSUPPORTED: "unsupported size",
+                 NEGF_ERR_CUDA: "CUDA error"}
+        raise NegfError(f"{what} failed: {names.get(code, code)}")
+
+
+def require_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        raise NegfError("dpnegf_b200 needs a CUDA device (B200, sm_100a); no CPU fallback exists")
+    load()
+
+
+def stream_handle(torch_stream=None):
+    import torch
+    s = torch_stream if torch_stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)

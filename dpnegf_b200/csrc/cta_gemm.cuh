@@ -1,0 +1,215 @@
+// CTA-wide complex128 GEMM on FP64 tensor cores (DMMA m8n8k4), 3M products.
+//
+//   C[M x N] = alpha * op(A) * op(B) + beta * D        (D may alias C)
+//
+// One CTA of 256 threads (8 warps) walks the 64x64 output tiles of C; each
+// tile streams 16-wide k-slabs of op(A) and op(B) into padded shared-memory
+// tiles with cp.async (double buffered).  Each warp owns a 32x16 sub-tile and
+// forms every complex product with three real DMMAs (Gauss/3M):
+//   T1 = Ar*Br, T2 = Ai*Bi, T3 = (Ar+Ai)*(Br+Bi);  Re = T1-T2, Im = T3-T1-T2.
+// Shared-memory pitches are chosen so the DMMA fragment reads (one 16-byte
+// complex per lane) are bank-conflict free for every operand orientation.
+#pragma once
+#include <type_traits>
+#include "negf_common.cuh"
+
+namespace negf {
+
+constexpr int GT_M = 64, GT_N = 64, GT_K = 16;
+constexpr int PITCH_MK = GT_K + 4;  // [64 rows][16 k] tiles (pitch = 4 mod 8)
+constexpr int PITCH_KN = GT_N + 2;  // [16 k][64 cols] tiles (pitch = 2 mod 8)
+constexpr int GT_TILE = (GT_M * PITCH_MK > GT_K * PITCH_KN) ? GT_M * PITCH_MK : GT_K * PITCH_KN;
+constexpr int GEMM_SMEM_BYTES = 4 * GT_TILE * (int)sizeof(cplx);  // 2 stages x (A,B)
+constexpr int CTA_THREADS = 256;
+
+struct GemmArgs {
+  int M, N, K;
+  const cplx* A;
+  int64_t lda;
+  const cplx* B;
+  int64_t ldb;
+  cplx* C;
+  int64_t ldc;
+  const cplx* D;  // addend, read only when use_d
+  int64_t ldd;
+  cplx alpha, beta;
+  bool use_d;
+};
+
+NEGF_DEV GemmArgs gemm_args(int M, int N, int K, const cplx* A, int64_t lda, const cplx* B, int64_t ldb,
+                            cplx* C, int64_t ldc) {
+  GemmArgs g;
+  g.M = M; g.N = N; g.K = K;
+  g.A = A; g.lda = lda; g.B = B; g.ldb = ldb; g.C = C; g.ldc = ldc;
+  g.D = nullptr; g.ldd = 0;
+  g.alpha = cmk(1.0, 0.0); g.beta = cmk(0.0, 0.0); g.use_d = false;
+  return g;
+}
+
+// op(A) tile element (m, k) -> shared-memory index
+template <int OP>
+NEGF_DEV int a_idx(int m, int k) { return OP == OP_C ? k * PITCH_KN + m : m * PITCH_MK + k; }
+// op(B) tile element (k, n) -> shared-memory index
+template <int OP>
+NEGF_DEV int b_idx(int k, int n) { return OP == OP_C ? n * PITCH_MK + k : k * PITCH_KN + n; }
+
+// Stage the (m0,k0) tile of op(A) into sA.
+template <int OP>
+NEGF_DEV void load_a_tile(cplx* sA, const GemmArgs& g, int m0, int k0, int tid) {
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    int e = tid + s * CTA_THREADS;
+    if (OP == OP_C) {  // stored X is K x M: tile rows k, cols m
+      int r = e >> 6, c = e & 63;
+      int k = k0 + r, m = m0 + c;
+      bool v = (k < g.K) && (m < g.M);
+      const cplx* src = v ? g.A + (int64_t)k * g.lda + m : g.A;
+      cp_async16(sA + r * PITCH_KN + c, src, v);
+    } else {  // stored A is M x K: tile rows m, cols k
+      int r = e >> 4, c = e & 15;
+      int m = m0 + r, k = k0 + c;
+      bool v = (m < g.M) && (k < g.K);
+      const cplx* src = v ? g.A + (int64_t)m * g.lda + k : g.A;
+      cp_async16(sA + r * PITCH_MK + c, src, v);
+    }
+  }
+}
+
+// Stage the (k0,n0) tile of op(B) into sB.
+template <int OP>
+NEGF_DEV void load_b_tile(cplx* sB, const GemmArgs& g, int k0, int n0, int tid) {
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    int e = tid + s * CTA_THREADS;
+    if (OP == OP_C) {  // stored X is N x K: tile rows n, cols k
+      int r = e >> 4, c = e & 15;
+      int n = n0 + r, k = k0 + c;
+      bool v = (n < g.N) && (k < g.K);
+      const cplx* src = v ? g.B + (int64_t)n * g.ldb + k : g.B;
+      cp_async16(sB + r * PITCH_MK + c, src, v);
+    } else {  // stored B is K x N: tile rows k, cols n
+      int r = e >> 6, c = e & 63;
+      int k = k0 + r, n = n0 + c;
+      bool v = (k < g.K) && (n < g.N);
+      const cplx* src = v ? g.B + (int64_t)k * g.ldb + n : g.B;
+      cp_async16(sB + r * PITCH_KN + c, src, v);
+    }
+  }
+}
+
+struct Acc3M {
+  double t1[4][2][2], t2[4][2][2], t3[4][2][2];
+  NEGF_DEV void zero() {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) t1[i][j][e] = t2[i][j][e] = t3[i][j][e] = 0.0;
+  }
+};
+
+// One warp: ksteps x (k=4) slabs of its 32x16 sub-tile.  Fragment reads go
+// through the index functors so the same loop serves the GEMM tiles and the
+// Gauss-Jordan panel update.
+template <bool CONJ_A, bool CONJ_B, class AIdx, class BIdx>
+NEGF_DEV void warp_mma_3m(Acc3M& acc, const cplx* sA, const cplx* sB, int ksteps, int wm, int wn, int lane,
+                          AIdx aidx, BIdx bidx) {
+  const int gr = lane >> 2, gc = lane & 3;
+  for (int ks = 0; ks < ksteps; ++ks) {
+    const int kk = ks * 4 + gc;
+    double ar[4], ai[4], as[4], br[2], bi[2], bs[2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      cplx a = sA[aidx(wm + i * 8 + gr, kk)];
+      ar[i] = a.x;
+      ai[i] = CONJ_A ? -a.y : a.y;
+      as[i] = ar[i] + ai[i];
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      cplx b = sB[bidx(kk, wn + j * 8 + gr)];
+      br[j] = b.x;
+      bi[j] = CONJ_B ? -b.y : b.y;
+      bs[j] = br[j] + bi[j];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        dmma884(acc.t1[i][j][0], acc.t1[i][j][1], ar[i], br[j]);
+        dmma884(acc.t2[i][j][0], acc.t2[i][j][1], ai[i], bi[j]);
+        dmma884(acc.t3[i][j][0], acc.t3[i][j][1], as[i], bs[j]);
+      }
+  }
+}
+
+// Visit every accumulator element of this warp: f(row, col, value).
+template <class F>
+NEGF_DEV void acc_foreach(const Acc3M& acc, int wm, int wn, int lane, F f) {
+  const int gr = lane >> 2, gc = lane & 3;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        double t1 = acc.t1[i][j][e], t2 = acc.t2[i][j][e], t3 = acc.t3[i][j][e];
+        f(wm + i * 8 + gr, wn + j * 8 + 2 * gc + e, cmk(t1 - t2, t3 - t1 - t2));
+      }
+}
+
+struct AIdxOp0 { NEGF_DEV int operator()(int m, int k) const { return a_idx<OP_N>(m, k); } };
+struct AIdxOpC { NEGF_DEV int operator()(int m, int k) const { return a_idx<OP_C>(m, k); } };
+struct BIdxOp0 { NEGF_DEV int operator()(int k, int n) const { return b_idx<OP_N>(k, n); } };
+struct BIdxOpC { NEGF_DEV int operator()(int k, int n) const { return b_idx<OP_C>(k, n); } };
+
+// C = alpha op(A) op(B) + beta D over the whole matrix, by the whole CTA.
+// C must not alias A or B.  Ends with __syncthreads(), so C is visible to
+// every thread of the CTA on return.
+template <int OPA, int OPB>
+NEGF_DEV void cta_gemm(const GemmArgs& g, cplx* smem) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = (warp >> 2) * 32, wn = (warp & 3) * 16;
+  cplx* sA[2] = {smem, smem + GT_TILE};
+  cplx* sB[2] = {smem + 2 * GT_TILE, smem + 3 * GT_TILE};
+  const int nk = (g.K + GT_K - 1) / GT_K;
+  typedef typename std::conditional<OPA == OP_C, AIdxOpC, AIdxOp0>::type AI;
+  typedef typename std::conditional<OPB == OP_C, BIdxOpC, BIdxOp0>::type BI;
+  constexpr bool CA = (OPA != OP_N), CB = (OPB != OP_N);
+
+  for (int m0 = 0; m0 < g.M; m0 += GT_M) {
+    for (int n0 = 0; n0 < g.N; n0 += GT_N) {
+      Acc3M acc;
+      acc.zero();
+      if (nk > 0) {
+        load_a_tile<OPA>(sA[0], g, m0, 0, tid);
+        load_b_tile<OPB>(sB[0], g, 0, n0, tid);
+      }
+      cp_async_commit();
+      for (int kt = 0; kt < nk; ++kt) {
+        if (kt + 1 < nk) {
+          load_a_tile<OPA>(sA[(kt + 1) & 1], g, m0, (kt + 1) * GT_K, tid);
+          load_b_tile<OPB>(sB[(kt + 1) & 1], g, (kt + 1) * GT_K, n0, tid);
+        }
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        warp_mma_3m<CA, CB>(acc, sA[kt & 1], sB[kt & 1], GT_K / 4, wm, wn, lane, AI(), BI());
+        __syncthreads();
+      }
+      acc_foreach(acc, wm, wn, lane, [&](int r, int c, cplx v) {
+        int m = m0 + r, n = n0 + c;
+        if (m < g.M && n < g.N) {
+          cplx o = cmul(g.alpha, v);
+          if (g.use_d) o = cfma(g.beta, g.D[(int64_t)m * g.ldd + n], o);
+          g.C[(int64_t)m * g.ldc + n] = o;
+        }
+      });
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+}
+
+}  // namespace negf

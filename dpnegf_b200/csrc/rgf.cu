@@ -1,0 +1,408 @@
+// Batched block-tridiagonal recursive Green's function (RGF) sweep, sm_100a.
+//
+// Persistent kernel: one CTA per work slot pulls (device, energy) items from
+// an atomic queue and runs the whole sweep for that item -- forward
+// left-connected inverses, backward retarded blocks, optional lesser blocks,
+// and the T(E) / per-orbital DOS reductions -- keeping its intermediates in a
+// private scratch slot.  All contractions go through the CTA tile GEMM and the
+// blocked Gauss-Jordan inverse on FP64 tensor cores (cta_gemm.cuh,
+// cta_inverse.cuh).
+//
+// Follows negf/recursive_green_cal.py (dpnegf):
+//   forward   g_0 = (-D_0)^-1,  g_q = (-D_q - L_{q-1} g_{q-1} U_{q-1})^-1     :88-94
+//   backward  gU = g_q U_q;  G_{q+1,q} = G_{q+1,q+1} L_q g_q;
+//             G_{q,q+1} = gU G_{q+1,q+1};  G_qq = g_q + gU G_{q+1,q};
+//             G_{q,N} = gU G_{q+1,N}                                           :98-114
+//   lesser    gin_0 = g_0 s_0 g_0^H;  gin_{q+1} = g_{q+1}(s_{q+1} + L gin_q U) g_{q+1}^H
+//             gnl_q = G_{q+1,q+1} L gin_q + gnd_{q+1} L g_q^H
+//             gnd_q = gin_q + g_q U gnd_{q+1} L g_q^H + gin_q U G_{q,q+1}^H
+//                     + G_{q,q+1} L gin_q;  gnu_q = gnl_q^H                      :121-140
+// with D = H + Sigma - zS, L = hl - z sl, U = hu - z su (:75-78), and the
+// reductions of negf/device_property.py: T = Re Tr[G_L G_1N G_R G_1N^H]
+// (:374-406) and -Im diag(G_qq S_qq + G_{q,q+1} S_{q+1,q} + G_{q,q-1} S_{q-1,q})/pi
+// per orbital (:408-470).
+#include <cstdio>
+#include "../../include/negf_b200.h"
+#include "cta_inverse.cuh"
+
+namespace negf {
+
+constexpr int RGF_NBUF = 18;  // per-slot max_n^2 work buffers (see SlotBufs)
+
+struct SlotBufs {
+  cplx* gslab;    // g_q storage when gr_left is not an output
+  cplx* ginslab;  // lesser gin_q storage when gin_left is not an output
+  cplx *W, *T1, *Lz, *Uz, *gU, *Gd, *Gl, *Gu, *Gt0, *Gt1, *tA, *tB, *tC, *tD;
+  cplx *Nd, *Nl, *Nu, *tE;  // lesser work
+};
+
+__host__ __device__ inline size_t rgf_slot_elems(const NegfRgfProblem& p) {
+  size_t mn2 = (size_t)p.max_n * p.max_n;
+  size_t e = RGF_NBUF * mn2;
+  if (!(p.flags & NEGF_OUT_GR_LEFT)) e += (size_t)p.max_g_slab;
+  if (p.flags & NEGF_LESSER) e += (size_t)p.max_g_slab;
+  return (e + 15) & ~(size_t)15;  // keep slots 256-byte aligned
+}
+constexpr size_t RGF_SCRATCH_HEADER = 256;  // work-queue counter
+
+NEGF_DEV SlotBufs slot_bufs(const NegfRgfProblem& p, int slot) {
+  cplx* base = reinterpret_cast<cplx*>(reinterpret_cast<char*>(p.scratch) + RGF_SCRATCH_HEADER) +
+               (size_t)slot * rgf_slot_elems(p);
+  size_t mn2 = (size_t)p.max_n * p.max_n;
+  SlotBufs s;
+  cplx* b = base;
+  cplx** bufs[RGF_NBUF] = {&s.W, &s.T1, &s.Lz, &s.Uz, &s.gU, &s.Gd, &s.Gl, &s.Gu, &s.Gt0,
+                           &s.Gt1, &s.tA, &s.tB, &s.tC, &s.tD, &s.Nd, &s.Nl, &s.Nu, &s.tE};
+  for (int i = 0; i < RGF_NBUF; ++i) { *bufs[i] = b; b += mn2; }
+  s.gslab = nullptr;
+  s.ginslab = nullptr;
+  if (!(p.flags & NEGF_OUT_GR_LEFT)) { s.gslab = b; b += p.max_g_slab; }
+  if (p.flags & NEGF_LESSER) { s.ginslab = b; b += p.max_g_slab; }
+  return s;
+}
+
+// Out = X - z Y  ([m x n]); a missing X or Y (offset -1) is a zero block.
+NEGF_DEV void form_shift(cplx* out, const cplx* hs, int64_t ox, int64_t oy, cplx z, int m, int n) {
+  const int tid = threadIdx.x;
+  for (int e = tid; e < m * n; e += CTA_THREADS) {
+    cplx x = ox >= 0 ? hs[ox + e] : cmk(0.0, 0.0);
+    cplx y = oy >= 0 ? hs[oy + e] : cmk(0.0, 0.0);
+    out[e] = csub(x, cmul(z, y));
+  }
+}
+
+// W = z S - H - (Sigma_L in the top-left corner) - (Sigma_R in the bottom-right
+// corner); the corner rule is recursive_green_cal.py:411-428.
+NEGF_DEV void form_a0(cplx* W, const cplx* hs, const NegfBlock& b, cplx z, const cplx* seL, int nsl,
+                      const cplx* seR, int nsr) {
+  const int n = b.n, tid = threadIdx.x;
+  const int cl = seL ? min(n, nsl) : 0;
+  const int cr = seR ? min(n, nsr) : 0;
+  for (int e = tid; e < n * n; e += CTA_THREADS) {
+    int i = e / n, j = e % n;
+    cplx v = csub(cmul(z, hs[b.sd + e]), hs[b.hd + e]);
+    if (i < cl && j < cl) v = csub(v, seL[(int64_t)i * nsl + j]);
+    if (i >= n - cr && j >= n - cr) {
+      int ii = i - (n - cr) + (nsr - cr), jj = j - (n - cr) + (nsr - cr);
+      v = csub(v, seR[(int64_t)ii * nsr + jj]);
+    }
+    W[e] = v;
+  }
+}
+
+NEGF_DEV void copy_mat(cplx* dst, const cplx* src, int m, int n) {
+  for (int e = threadIdx.x; e < m * n; e += CTA_THREADS) dst[e] = src[e];
+}
+
+// dst[i] (+)= -Im( sum_j A[i][j] B[j][i] ) / pi   (A: rows x inner, B: inner x rows)
+NEGF_DEV void diag_im_acc(double* dst, const cplx* A, const cplx* B, int rows, int inner, bool init) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int i = warp; i < rows; i += CTA_THREADS / 32) {
+    double acc = 0.0;
+    for (int j = lane; j < inner; j += 32) {
+      cplx a = A[(int64_t)i * inner + j], b = B[(int64_t)j * rows + i];
+      acc += a.x * b.y + a.y * b.x;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if (lane == 0) {
+      double v = -acc * 0.31830988618379067154;  // 1/pi
+      dst[i] = init ? v : dst[i] + v;
+    }
+  }
+}
+
+// Gamma = i (Sigma - Sigma^H) on the c x c corner of Sigma (ns x ns) at (r0, r0).
+NEGF_DEV void form_gamma(cplx* out, const cplx* se, int ns, int r0, int c) {
+  for (int e = threadIdx.x; e < c * c; e += CTA_THREADS) {
+    int i = e / c, k = e % c;
+    cplx a = se[(int64_t)(r0 + i) * ns + r0 + k], b = se[(int64_t)(r0 + k) * ns + r0 + i];
+    cplx d = csub(a, cconj(b));
+    out[e] = cmk(-d.y, d.x);
+  }
+}
+
+NEGF_DEV double cta_sum(double v, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int w = 0; w < CTA_THREADS / 32; ++w) s += red[w];
+  __syncthreads();
+  return s;
+}
+
+template <int OPA, int OPB>
+NEGF_DEV void gemm(cplx* smem, int M, int N, int K, const cplx* A, int64_t lda, const cplx* B, int64_t ldb,
+                   cplx* C, int64_t ldc, cplx alpha = cmk(1.0, 0.0), const cplx* D = nullptr,
+                   int64_t ldd = 0, cplx beta = cmk(1.0, 0.0)) {
+  GemmArgs g = gemm_args(M, N, K, A, lda, B, ldb, C, ldc);
+  g.alpha = alpha;
+  if (D) { g.D = D; g.ldd = ldd; g.beta = beta; g.use_d = true; }
+  cta_gemm<OPA, OPB>(g, smem);
+}
+
+NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBufs& sb, char* smem_raw,
+                       double* red) {
+  cplx* smem = reinterpret_cast<cplx*>(smem_raw);
+  const NegfDevice dv = P.devices[it.dev];
+  const NegfBlock* blk = P.blocks + dv.blk0;
+  const int K = dv.n_blocks;
+  const int row = it.row;
+  const uint32_t fl = P.flags;
+  const cplx z = cmk(it.z_re, it.z_im);
+  const cplx* hs = reinterpret_cast<const cplx*>(P.hs);
+  const cplx* se = reinterpret_cast<const cplx*>(P.se);
+  const cplx* sin = reinterpret_cast<const cplx*>(P.s_in);
+  cplx* out = reinterpret_cast<cplx*>(P.out);
+  const cplx* seL = it.se_l >= 0 ? se + it.se_l : nullptr;
+  const cplx* seR = it.se_r >= 0 ? se + it.se_r : nullptr;
+  const cplx ONE = cmk(1.0, 0.0), MONE = cmk(-1.0, 0.0);
+  const bool lesser = (fl & NEGF_LESSER) != 0;
+  int bad = 0;
+
+  auto sq = [&](int q) { return (int64_t)blk[q].n * blk[q].n; };
+  auto gptr = [&](int q) -> cplx* {
+    return (fl & NEGF_OUT_GR_LEFT) ? out + blk[q].o_grleft + row * sq(q) : sb.gslab + blk[q].g;
+  };
+  auto ginptr = [&](int q) -> cplx* {
+    return blk[q].o_ginleft >= 0 ? out + blk[q].o_ginleft + row * sq(q) : sb.ginslab + blk[q].g;
+  };
+  auto sinptr = [&](int q) -> const cplx* {
+    return blk[q].s_in >= 0 ? sin + blk[q].s_in + row * sq(q) : nullptr;
+  };
+
+  // ------------------------------------------------------------ forward sweep
+  for (int q = 0; q < K; ++q) {
+    const NegfBlock& b = blk[q];
+    const int nq = b.n;
+    form_a0(sb.W, hs, b, z, q == 0 ? seL : nullptr, it.nse_l, q == K - 1 ? seR : nullptr, it.nse_r);
+    if (q > 0) {
+      const NegfBlock& bp = blk[q - 1];
+      const int np = bp.n;
+      form_shift(sb.Lz, hs, bp.hl, bp.sl, z, nq, np);  // L_{q-1}: n_q x n_{q-1}
+      form_shift(sb.Uz, hs, bp.hu, bp.su, z, np, nq);  // U_{q-1}: n_{q-1} x n_q
+      __syncthreads();
+      gemm<OP_N, OP_N>(smem, nq, np, np, sb.Lz, np, gptr(q - 1), np, sb.T1, np);
+      gemm<OP_N, OP_N>(smem, nq, nq, np, sb.T1, np, sb.Uz, nq, sb.W, nq, MONE, sb.W, nq);
+    } else {
+      __syncthreads();
+    }
+    bad |= cta_inverse(sb.W, nq, nq, gptr(q), nq, smem_raw);
+    if (lesser) {
+      // gin_q = g_q (s_q + L gin_{q-1} U) g_q^H
+      const cplx* s = sinptr(q);
+      if (q > 0) {
+        const int np = blk[q - 1].n;
+        gemm<OP_N, OP_N>(smem, nq, np, np, sb.Lz, np, ginptr(q - 1), np, sb.T1, np);
+        if (s) gemm<OP_N, OP_N>(smem, nq, nq, np, sb.T1, np, sb.Uz, nq, sb.tA, nq, ONE, s, nq);
+        else gemm<OP_N, OP_N>(smem, nq, nq, np, sb.T1, np, sb.Uz, nq, sb.tA, nq);
+      } else {
+        if (s) copy_mat(sb.tA, s, nq, nq);
+        else for (int e = threadIdx.x; e < nq * nq; e += CTA_THREADS) sb.tA[e] = cmk(0.0, 0.0);
+        __syncthreads();
+      }
+      gemm<OP_N, OP_N>(smem, nq, nq, nq, gptr(q), nq, sb.tA, nq, sb.tB, nq);
+      gemm<OP_N, OP_C>(smem, nq, nq, nq, sb.tB, nq, gptr(q), nq, ginptr(q), nq);
+    }
+  }
+
+  // ----------------------------------------------------------- backward sweep
+  const int nN = blk[K - 1].n;
+  const bool need_gt = (fl & (NEGF_OUT_GTRANS | NEGF_OUT_GR_LC | NEGF_TRANS)) != 0;
+  double* orb = (fl & NEGF_ORB_DOS) ? P.orb_dos + it.orb : nullptr;
+
+  const cplx* Gnext = gptr(K - 1);
+  if (fl & NEGF_OUT_GRD) {
+    cplx* d = out + blk[K - 1].o_grd + row * sq(K - 1);
+    copy_mat(d, gptr(K - 1), nN, nN);
+    Gnext = d;
+  }
+  const cplx* gt = gptr(K - 1);
+  if (fl & NEGF_OUT_GR_LC) {
+    cplx* d = out + blk[K - 1].o_grlc + row * sq(K - 1);
+    copy_mat(d, gptr(K - 1), nN, nN);
+    gt = d;
+  }
+  const cplx* Nnext = nullptr;  // gnd_{q+1}
+  if (lesser) {
+    Nnext = ginptr(K - 1);
+    if (blk[K - 1].o_gnd >= 0) {
+      cplx* d = out + blk[K - 1].o_gnd + row * sq(K - 1);
+      copy_mat(d, ginptr(K - 1), nN, nN);
+      Nnext = d;
+    }
+  }
+  __syncthreads();
+  if (orb) {
+    diag_im_acc(orb + blk[K - 1].orb0, gptr(K - 1), hs + blk[K - 1].sd, nN, nN, true);
+    __syncthreads();
+  }
+  int tog = 0;
+  for (int q = K - 2; q >= 0; --q) {
+    const NegfBlock& b = blk[q];
+    const int nq = b.n, nn = b.n_next;
+    const int64_t szu = (int64_t)nq * nn;
+    form_shift(sb.Lz, hs, b.hl, b.sl, z, nn, nq);  // L_q: n_{q+1} x n_q
+    form_shift(sb.Uz, hs, b.hu, b.su, z, nq, nn);  // U_q: n_q x n_{q+1}
+    __syncthreads();
+    const cplx* g = gptr(q);
+    cplx* grl = (fl & NEGF_OUT_GRL) ? out + b.o_grl + row * szu : sb.Gl;
+    cplx* gru = (fl & NEGF_OUT_GRU) ? out + b.o_gru + row * szu : sb.Gu;
+    cplx* grd = (fl & NEGF_OUT_GRD) ? out + b.o_grd + row * sq(q) : sb.Gd;
+    gemm<OP_N, OP_N>(smem, nq, nn, nq, g, nq, sb.Uz, nn, sb.gU, nn);         // gU = g U
+    gemm<OP_N, OP_N>(smem, nn, nq, nn, Gnext, nn, sb.Lz, nq, sb.T1, nq);     // G_{q+1,q+1} L
+    gemm<OP_N, OP_N>(smem, nn, nq, nq, sb.T1, nq, g, nq, grl, nq);           // grl
+    gemm<OP_N, OP_N>(smem, nq, nn, nn, sb.gU, nn, Gnext, nn, gru, nn);       // gru
+    gemm<OP_N, OP_N>(smem, nq, nq, nn, sb.gU, nn, grl, nq, grd, nq, ONE, g, nq);  // grd
+    if (need_gt) {
+      cplx* gtn = (fl & NEGF_OUT_GR_LC) ? out + b.o_grlc + row * (int64_t)nq * nN : (tog ? sb.Gt1 : sb.Gt0);
+      gemm<OP_N, OP_N>(smem, nq, nN, nn, sb.gU, nn, gt, nN, gtn, nN);
+      gt = gtn;
+      tog ^= 1;
+    }
+    if (lesser) {
+      const cplx* gin = ginptr(q);
+      cplx* gnl = b.o_gnl >= 0 ? out + b.o_gnl + row * szu : sb.Nl;
+      cplx* gnd = b.o_gnd >= 0 ? out + b.o_gnd + row * sq(q) : sb.Nd;
+      // gLmH = L g^H  (n_{q+1} x n_q)
+      gemm<OP_N, OP_C>(smem, nn, nq, nq, sb.Lz, nq, g, nq, sb.tA, nq);
+      // gnl = G_{q+1,q+1} L gin + gnd_{q+1} gLmH ; sb.T1 still holds G_{q+1,q+1} L
+      gemm<OP_N, OP_N>(smem, nn, nq, nn, Nnext, nn, sb.tA, nq, sb.tB, nq);
+      gemm<OP_N, OP_N>(smem, nn, nq, nq, sb.T1, nq, gin, nq, gnl, nq, ONE, sb.tB, nq);
+      // gnd = gin + (g U) gnd_{q+1} gLmH + gin U gru^H + gru L gin
+      gemm<OP_N, OP_N>(smem, nq, nq, nn, sb.gU, nn, sb.tB, nq, sb.tC, nq, ONE, gin, nq);
+      gemm<OP_N, OP_N>(smem, nq, nn, nq, gin, nq, sb.Uz, nn, sb.tD, nn);
+      gemm<OP_N, OP_C>(smem, nq, nq, nn, sb.tD, nn, gru, nn, sb.tC, nq, ONE, sb.tC, nq);
+      gemm<OP_N, OP_N>(smem, nq, nq, nn, gru, nn, sb.Lz, nq, sb.tE, nq);
+      gemm<OP_N, OP_N>(smem, nq, nq, nq, sb.tE, nq, gin, nq, gnd, nq, ONE, sb.tC, nq);
+      if (b.o_gnu >= 0) {
+        cplx* gnu = out + b.o_gnu + row * szu;
+        for (int e = threadIdx.x; e < nq * nn; e += CTA_THREADS) {
+          int i = e / nn, j = e % nn;  // gnu[i][j] = conj(gnl[j][i])
+          gnu[e] = cconj(gnl[(int64_t)j * nq + i]);
+        }
+      }
+      __syncthreads();
+      Nnext = gnd;
+    }
+    if (orb) {
+      diag_im_acc(orb + b.orb0, grd, hs + b.sd, nq, nq, true);
+      __syncthreads();
+      if (b.sl >= 0) { diag_im_acc(orb + b.orb0, gru, hs + b.sl, nq, nn, false); __syncthreads(); }
+      if (b.su >= 0) { diag_im_acc(orb + blk[q + 1].orb0, grl, hs + b.su, nn, nq, false); __syncthreads(); }
+    }
+    Gnext = grd;
+  }
+  if (fl & NEGF_OUT_GTRANS) {
+    cplx* d = out + dv.o_gtrans + row * (int64_t)blk[0].n * nN;
+    copy_mat(d, gt, blk[0].n, nN);
+    __syncthreads();
+  }
+
+  // ------------------------------------------------------------ T(E)
+  double tval = 0.0;
+  if ((fl & NEGF_TRANS) && seL && seR) {
+    const int n0 = blk[0].n;
+    const int cl = min(n0, it.nse_l), cr = min(nN, it.nse_r);
+    const cplx* Gc = gt + (nN - cr);  // G_1N[0:cl, nN-cr:nN], row stride nN
+    form_gamma(sb.tA, seL, it.nse_l, 0, cl);
+    form_gamma(sb.tB, seR, it.nse_r, it.nse_r - cr, cr);
+    __syncthreads();
+    gemm<OP_N, OP_N>(smem, cl, cr, cl, sb.tA, cl, Gc, nN, sb.tC, cr);   // Gamma_L G
+    gemm<OP_N, OP_N>(smem, cl, cr, cr, sb.tC, cr, sb.tB, cr, sb.tD, cr);  // ... Gamma_R
+    double part = 0.0;
+    for (int e = threadIdx.x; e < cl * cr; e += CTA_THREADS) {
+      int i = e / cr, l = e % cr;
+      cplx a = sb.tD[e], gg = Gc[(int64_t)i * nN + l];
+      part += a.x * gg.x + a.y * gg.y;  // Re(a conj(g))
+    }
+    tval = cta_sum(part, red);
+  }
+  if (threadIdx.x == 0) {
+    if (fl & NEGF_TRANS) P.trans[it.out] = tval;
+    int st = NEGF_OK;
+    if (bad) st = NEGF_ERR_SINGULAR;
+    else if (!isfinite(tval)) st = NEGF_ERR_NONFINITE;
+    P.status[it.out] = st;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(CTA_THREADS, 1) rgf_kernel(const NegfRgfProblem P) {
+  extern __shared__ __align__(16) char smem[];
+  __shared__ int s_item;
+  __shared__ double red[CTA_THREADS / 32];
+  unsigned* queue = reinterpret_cast<unsigned*>(P.scratch);
+  const SlotBufs sb = slot_bufs(P, blockIdx.x);
+  for (;;) {
+    if (threadIdx.x == 0) s_item = (int)atomicAdd(queue, 1u);
+    __syncthreads();
+    const int idx = s_item;
+    __syncthreads();
+    if (idx >= P.n_items) break;
+    const NegfItem it = P.items[idx];
+    rgf_item(P, it, sb, smem, red);
+  }
+}
+
+size_t rgf_smem_bytes(int max_n) {
+  size_t a = GEMM_SMEM_BYTES, b = inv_smem_bytes_host(max_n);
+  return a > b ? a : b;
+}
+
+}  // namespace negf
+
+extern "C" {
+
+size_t negf_rgf_scratch_bytes(const NegfRgfProblem* p) {
+  if (!p || p->n_slots <= 0 || p->max_n <= 0) return 0;
+  return negf::RGF_SCRATCH_HEADER + (size_t)p->n_slots * negf::rgf_slot_elems(*p) * sizeof(double2);
+}
+
+int negf_rgf_run(const NegfRgfProblem* p, void* stream) {
+  if (!p || !p->blocks || !p->devices || !p->items || !p->hs || !p->status || !p->scratch) return NEGF_ERR_ARGUMENT;
+  if (p->n_items <= 0) return NEGF_OK;
+  if (p->max_n <= 0 || p->n_slots <= 0) return NEGF_ERR_ARGUMENT;
+  if (p->max_n > NEGF_MAX_BLOCK) return NEGF_ERR_UNSUPPORTED;
+  if (p->scratch_bytes < negf_rgf_scratch_bytes(p)) return NEGF_ERR_ARGUMENT;
+  if ((reinterpret_cast<uintptr_t>(p->scratch) & 255) != 0) return NEGF_ERR_ARGUMENT;
+  if ((p->flags & NEGF_TRANS) && !p->trans) return NEGF_ERR_ARGUMENT;
+  if ((p->flags & NEGF_ORB_DOS) && !p->orb_dos) return NEGF_ERR_ARGUMENT;
+  const uint32_t blockouts = NEGF_OUT_GTRANS | NEGF_OUT_GR_LC | NEGF_OUT_GRD | NEGF_OUT_GRL | NEGF_OUT_GRU |
+                             NEGF_OUT_GR_LEFT | NEGF_LESSER;
+  if ((p->flags & blockouts) && !p->out) return NEGF_ERR_ARGUMENT;
+  if ((p->flags & NEGF_LESSER) && !p->s_in) return NEGF_ERR_ARGUMENT;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const size_t smem = negf::rgf_smem_bytes(p->max_n);
+  if (cudaFuncSetAttribute(negf::rgf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return NEGF_ERR_CUDA;
+  if (cudaMemsetAsync(p->scratch, 0, negf::RGF_SCRATCH_HEADER, s) != cudaSuccess) return NEGF_ERR_CUDA;
+  const int grid = p->n_slots < p->n_items ? p->n_slots : p->n_items;
+  negf::rgf_kernel<<<grid, negf::CTA_THREADS, smem, s>>>(*p);
+  return cudaGetLastError() == cudaSuccess ? NEGF_OK : NEGF_ERR_CUDA;
+}
+
+int negf_sm_count(void) {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
+  return n;
+}
+
+const char* negf_version(void) { return "negf_b200 0.1.0 (sm_100a)"; }
+
+size_t negf_abi_struct_size(int which) {
+  switch (which) {
+    case 0: return sizeof(NegfBlock);
+    case 1: return sizeof(NegfDevice);
+    case 2: return sizeof(NegfItem);
+    case 3: return sizeof(NegfRgfProblem);
+    default: return 0;
+  }
+}
+
+}  // extern "C"

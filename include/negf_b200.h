@@ -1,0 +1,140 @@
+/*
+ * negf_b200.h -- C ABI of the B200-native NEGF transport core.
+ *
+ * Every entry point takes plain pointers and sizes.  All array pointers in the
+ * problem descriptors are DEVICE pointers (cudaMalloc'd or torch-owned CUDA
+ * memory) unless a field says otherwise; complex numbers are complex128
+ * stored interleaved (re, im) -- the layout of torch.complex128 / numpy
+ * complex128, so caller tensors are passed without conversion.  Calls are
+ * asynchronous on the given stream and allocate no device memory: scratch is
+ * supplied by the caller (size from the matching *_scratch_bytes query).
+ *
+ * Offsets named "offset" count complex elements (16 bytes), not bytes.
+ *
+ * Reference interfaces replaced (dpnegf, paths relative to its source tree):
+ *   negf_rgf_run           negf/recursive_green_cal.py:4-296  recursive_gf_cal
+ *                          (called by recursive_gf :324-477), fused with the
+ *                          T(E) / DOS / LDOS reductions of
+ *                          negf/device_property.py:374-470
+ *   negf_lopez_sancho_run  negf/surface_green.py:102-159  _surface_green_numba_core
+ *                          + the self-energy product of selfEnergy :9-91
+ */
+#ifndef NEGF_B200_H
+#define NEGF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (per call and per work item) ------------------------- */
+#define NEGF_OK 0
+#define NEGF_WARN_LS_CONVERGENCE 1 /* Lopez-Sancho residual in (1e-8, 3e-5): surface_green.py:149-150 */
+#define NEGF_ERR_LS_NOT_CONVERGED 2 /* > 100 decimation steps: surface_green.py:156-157 (RuntimeError) */
+#define NEGF_ERR_LS_RESIDUAL 3      /* residual >= 3e-5: surface_green.py:154 (ArithmeticError) */
+#define NEGF_ERR_SINGULAR 4         /* zero / non-finite pivot (torch.linalg.solve raises) */
+#define NEGF_ERR_NONFINITE 5        /* non-finite result */
+#define NEGF_ERR_ARGUMENT -1        /* malformed descriptor (call-level) */
+#define NEGF_ERR_UNSUPPORTED -2     /* block size above the compiled maximum (call-level) */
+#define NEGF_ERR_CUDA -3            /* CUDA launch / attribute error (call-level) */
+
+#define NEGF_MAX_BLOCK 512 /* largest diagonal block the kernels accept */
+
+/* ---- RGF output selection (NegfRgfProblem.flags) ------------------------ */
+#define NEGF_OUT_GTRANS (1u << 0)  /* g_trans = G_{1N}           [n_0 x n_{K-1}] */
+#define NEGF_OUT_GR_LC (1u << 1)   /* gr_lc[q] = G_{q,N}         [n_q x n_{K-1}] */
+#define NEGF_OUT_GRD (1u << 2)     /* grd[q]  = G_{q,q}          [n_q x n_q]     */
+#define NEGF_OUT_GRL (1u << 3)     /* grl[q]  = G_{q+1,q}        [n_{q+1} x n_q] */
+#define NEGF_OUT_GRU (1u << 4)     /* gru[q]  = G_{q,q+1}        [n_q x n_{q+1}] */
+#define NEGF_OUT_GR_LEFT (1u << 5) /* gr_left[q] = g_q (left-connected) [n_q x n_q] */
+#define NEGF_TRANS (1u << 6)       /* T(E) = Re Tr[G_L G_1N G_R G_1N^H] -> trans[]  */
+#define NEGF_ORB_DOS (1u << 7)     /* -Im diag(G S)_i / pi per orbital -> orb_dos[] */
+#define NEGF_LESSER (1u << 8)      /* lesser sweep: gin_left, gnd, gnl, gnu          */
+
+/* One diagonal block q of a block-tridiagonal device. */
+typedef struct NegfBlock {
+  int32_t n;      /* n_q */
+  int32_t n_next; /* n_{q+1}; 0 for the last block */
+  int64_t hd, sd; /* offsets of H_qq, S_qq in hs */
+  int64_t hu, su; /* offsets of H_{q,q+1}, S_{q,q+1} [n_q x n_{q+1}]; -1 = zero block */
+  int64_t hl, sl; /* offsets of H_{q+1,q}, S_{q+1,q} [n_{q+1} x n_q]; -1 = zero block */
+  int64_t orb0;   /* first orbital of block q within its device */
+  int64_t g;      /* offset of g_q inside one item's g slab (prefix sum of n^2) */
+  /* block outputs: offset of batch row 0 in out; row b adds b * (block size).
+     -1 when not produced. */
+  int64_t o_grd, o_grl, o_gru, o_grlc, o_grleft;
+  int64_t o_gnd, o_gnl, o_gnu, o_ginleft;
+  int64_t s_in; /* lesser input Sigma^in_q for batch row 0 in s_in; -1 = zero */
+} NegfBlock;
+
+/* One device (k-point / realisation): a run of n_blocks NegfBlock entries. */
+typedef struct NegfDevice {
+  int32_t n_blocks; /* K */
+  int32_t blk0;     /* index of block 0 in the block table */
+  int32_t n_orb;    /* sum of n_q */
+  int32_t pad;
+  int64_t o_gtrans; /* g_trans for batch row 0 in out; -1 when not produced */
+  int64_t g_slab;   /* elements of one item's g slab (sum of n_q^2) */
+} NegfDevice;
+
+/* One work item: a device at one complex energy. */
+typedef struct NegfItem {
+  int32_t dev;     /* device index */
+  int32_t row;     /* batch row of this energy within the device's outputs */
+  double z_re;     /* z = E + E_ref + i*eta (recursive_green_cal.py:75,:378) */
+  double z_im;
+  int64_t se_l;    /* offset of Sigma_L [nse_l x nse_l] in se; -1 = none */
+  int64_t se_r;    /* offset of Sigma_R [nse_r x nse_r] in se; -1 = none */
+  int32_t nse_l, nse_r;
+  int64_t out;     /* index into trans[] and status[] */
+  int64_t orb;     /* offset (doubles) of this item's n_orb entries in orb_dos[] */
+} NegfItem;
+
+typedef struct NegfRgfProblem {
+  const NegfBlock* blocks;  /* device memory */
+  const NegfDevice* devices; /* device memory */
+  const NegfItem* items;    /* device memory, processed in this order */
+  int32_t n_items;
+  int32_t max_n;            /* largest n_q over all devices (<= NEGF_MAX_BLOCK) */
+  int64_t max_g_slab;       /* largest g slab over all devices */
+  const double* hs;         /* complex128 arena of H/S blocks */
+  const double* se;         /* complex128 arena of self-energies */
+  const double* s_in;       /* complex128 arena of Sigma^in blocks (NEGF_LESSER) */
+  double* out;              /* complex128 arena of block outputs */
+  double* trans;            /* [n_items] T(E) (NEGF_TRANS) */
+  double* orb_dos;          /* per-orbital -Im diag(GS)/pi (NEGF_ORB_DOS) */
+  int32_t* status;          /* [n_items] per-item status (always written) */
+  uint32_t flags;
+  int32_t n_slots;          /* concurrent work slots = CTAs launched */
+  void* scratch;            /* >= negf_rgf_scratch_bytes(problem) bytes, 256-aligned */
+  size_t scratch_bytes;
+} NegfRgfProblem;
+
+/* Bytes of scratch negf_rgf_run needs for p->n_slots, p->max_n, p->max_g_slab, p->flags. */
+size_t negf_rgf_scratch_bytes(const NegfRgfProblem* p);
+
+/* Batched RGF sweep over p->n_items (device, energy) items.  Replaces
+ * recursive_gf_cal (negf/recursive_green_cal.py:4-296): forward left-connected
+ * g_q = (-D_q - L_{q-1} g_{q-1} U_{q-1})^-1 with D = H + Sigma - zS, L = hl - z sl,
+ * U = hu - z su; backward G_qq, G_{q+1,q}, G_{q,q+1}, G_{q,N}; optional lesser
+ * sweep (:121-140).  T(E) (device_property.py:374-406) and the per-orbital DOS
+ * diagonal (:408-470) are reduced inside the sweep.  Returns a call-level
+ * status; per-item status in p->status. */
+int negf_rgf_run(const NegfRgfProblem* p, void* cuda_stream);
+
+/* Number of SMs of the current CUDA device (grid sizing helper). */
+int negf_sm_count(void);
+
+/* Library version string. */
+const char* negf_version(void);
+
+/* sizeof of the ABI structs (0 NegfBlock, 1 NegfDevice, 2 NegfItem,
+ * 3 NegfRgfProblem) so bindings can verify their mirrors; 0 if unknown. */
+size_t negf_abi_struct_size(int which);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NEGF_B200_H */

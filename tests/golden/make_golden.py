@@ -1,0 +1,249 @@
+"""Generate the golden fixtures in this directory by running the REFERENCE code.
+
+Run from the repository root in a container that has the dpnegf sources:
+
+    python tests/golden/make_golden.py [--ref-root PATH]
+
+It imports the reference hot path through ``oracle/ref_import.py`` and records
+seeded inputs together with the reference's own outputs:
+
+  rgf_*.npz       ``recursive_gf`` (negf/recursive_green_cal.py:324) retarded,
+                  lesser and greater cases, uniform and non-uniform blocks,
+                  batched and scalar energies;
+  devprop_*.npz   ``DeviceProperty.cal_green_function`` + ``_cal_tc_`` /
+                  ``_cal_dos_`` / ``_cal_ldos_`` (negf/device_property.py)
+                  driven through the same fakes the reference tests use;
+  lopez_*.npz     ``surface_green`` / ``selfEnergy`` (negf/surface_green.py)
+                  for the 1-D chain lead and a random non-orthogonal lead;
+  ozaki.npz       ``ozaki_residues`` (negf/ozaki_res_cal.py) and ``gauss_xw``
+                  (negf/negf_utils.py:136).
+The fixtures are small (tens of KB) and are committed; the GPU box never needs
+the reference sources.
+"""
+import argparse
+import os
+import sys
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import ref_import  # noqa: E402
+from dpnegf_b200 import workload  # noqa: E402
+
+
+def _put(d, key, val):
+    if val is None:
+        return
+    if isinstance(val, (list, tuple)):
+        d[f"{key}#len"] = np.array(len(val))
+        for i, v in enumerate(val):
+            _put(d, f"{key}/{i}", v)
+    else:
+        d[key] = val.detach().resolve_conj().cpu().numpy() if torch.is_tensor(val) else np.asarray(val)
+
+
+def _rgf_case(rgf_mod, name, dims, B, seed, lesser=False, greater=False, scalar=False,
+              gr_lc=True, eta=1e-5, E_ref=0.0):
+    dev = workload.random_device(0, 0, seed=seed, block_dims=dims)
+    seL = workload.random_self_energy(B, dims[0], seed=seed + 100)
+    seR = workload.random_self_energy(B, dims[-1], seed=seed + 200)
+    E = torch.linspace(-1.5, 1.5, B, dtype=torch.float64).to(torch.complex128)
+    s_in = s_out = 0
+    gen = torch.Generator().manual_seed(seed + 300)
+    if lesser:
+        s_in = []
+        for n in dims:
+            x = torch.complex(torch.randn(B, n, n, generator=gen, dtype=torch.float64),
+                              torch.randn(B, n, n, generator=gen, dtype=torch.float64))
+            s_in.append(0.5 * (x + x.mH))
+    if greater:
+        s_out = []
+        for n in dims:
+            x = torch.complex(torch.randn(B, n, n, generator=gen, dtype=torch.float64),
+                              torch.randn(B, n, n, generator=gen, dtype=torch.float64))
+            s_out.append(0.5 * (x + x.mH))
+    kw = dict(hl=dev.hl, hd=dev.hd, hu=dev.hu, sd=dev.sd, su=dev.su, sl=dev.sl, eta=eta,
+              E_ref=E_ref, need_lesser=lesser, need_greater=greater, need_gr_lc=gr_lc)
+    if scalar:
+        assert B == 1
+        ans = rgf_mod.recursive_gf(E[0], left_se=seL[0], right_se=seR[0],
+                                   s_in=[s[0] for s in s_in] if lesser else 0,
+                                   s_out=[s[0] for s in s_out] if greater else 0, **kw)
+    else:
+        ans = rgf_mod.recursive_gf(E, left_se=seL, right_se=seR, s_in=s_in, s_out=s_out, **kw)
+    d = {}
+    _put(d, "dims", np.array(dims))
+    _put(d, "energy", E)
+    _put(d, "eta", np.array(eta))
+    _put(d, "E_ref", np.array(E_ref))
+    _put(d, "scalar", np.array(scalar))
+    for k in ("hd", "hu", "hl", "sd", "su", "sl"):
+        _put(d, k, getattr(dev, k))
+    _put(d, "left_se", seL)
+    _put(d, "right_se", seR)
+    if lesser:
+        _put(d, "s_in", s_in)
+    if greater:
+        _put(d, "s_out", s_out)
+    tags = ("g_trans", "gr_lc", "grd", "grl", "gru", "gr_left",
+            "gnd", "gnl", "gnu", "gin_left", "gpd", "gpl", "gpu", "gip_left")
+    for t, v in zip(tags, ans):
+        _put(d, "out/" + t, v)
+    np.savez_compressed(os.path.join(HERE, f"rgf_{name}.npz"), **d)
+
+
+class _FakeHamiltonian:
+    def __init__(self, dev):
+        self._packed = (dev.hd, dev.sd, dev.hl, dev.su, dev.sl, dev.hu)
+        self.device_norbs = dev.norbs_per_atom
+
+    def get_hs_device(self, kpoint, V, block_tridiagonal):
+        return self._packed
+
+
+class _FakeLead:
+    def __init__(self, mu, kBT=0.025):
+        self.se = None
+        self.chemiPot_lead = mu
+        self.kBT = kBT
+
+    def fermi_dirac(self, x):
+        return 1.0 / (1.0 + torch.exp((x - self.chemiPot_lead) / self.kBT))
+
+    @property
+    def gamma(self):
+        return 1j * (self.se - self.se.mH)
+
+
+def _devprop_case(dp_mod, name, dims, B, seed, norbs, need_lesser=True):
+    dev = workload.random_device(0, 0, seed=seed, block_dims=dims)
+    dev.norbs_per_atom = norbs
+    seL = workload.random_self_energy(B, dims[0], seed=seed + 1)
+    seR = workload.random_self_energy(B, dims[-1], seed=seed + 2)
+    E = torch.linspace(-0.3, 0.4, B, dtype=torch.float64).to(torch.complex128)
+    dp = dp_mod.DeviceProperty.__new__(dp_mod.DeviceProperty)
+    dp.greenfuncs = 0
+    dp.hamiltonian = _FakeHamiltonian(dev)
+    dp.structure = None
+    dp.results_path = "/nonexistent-negf-results"
+    dp.cdtype = torch.complex128
+    dp.rgf_device = "cpu"
+    dp.kBT = 0.025
+    dp.e_T = 300.0
+    dp.chemiPot = None
+    dp.E_ref = 0.05
+    dp.kpoint = None
+    dp.newK_flag = None
+    dp.newV_flag = None
+    dp.lead_L = _FakeLead(0.1)
+    dp.lead_R = _FakeLead(-0.1)
+    dp.lead_L.se = seL
+    dp.lead_R.se = seR
+    dp.cal_green_function(energy=E, kpoint=[0.0, 0.0, 0.0], eta_device=1e-6,
+                          block_tridiagonal=True, need_lesser=need_lesser)
+    d = {}
+    _put(d, "dims", np.array(dims))
+    _put(d, "norbs", np.array(norbs))
+    _put(d, "energy", E)
+    for k in ("hd", "hu", "hl", "sd", "su", "sl"):
+        _put(d, k, getattr(dev, k))
+    _put(d, "left_se", seL)
+    _put(d, "right_se", seR)
+    _put(d, "E_ref", np.array(0.05))
+    _put(d, "eta_device", np.array(1e-6))
+    _put(d, "muL", np.array(0.1))
+    _put(d, "muR", np.array(-0.1))
+    _put(d, "kBT", np.array(0.025))
+    _put(d, "out/tc", dp._cal_tc_())
+    _put(d, "out/dos", dp._cal_dos_())
+    _put(d, "out/ldos", dp._cal_ldos_())
+    if need_lesser:
+        _put(d, "out/gnd", dp.greenfuncs["gnd"])
+    np.savez_compressed(os.path.join(HERE, f"devprop_{name}.npz"), **d)
+
+
+def _lopez_cases(sg_mod):
+    d = {}
+    chain = workload.chain_device(L=4)
+    ld = chain.lead_R
+    es = np.array([-2.5, -1.0, 0.0, 0.7, 1.9, 2.6])
+    gs_all, sig_all = [], []
+    for e in es:
+        gs = sg_mod.surface_green(ld.hL.numpy(), ld.hLL.numpy(), ld.sL.numpy(), ld.sLL.numpy(),
+                                  complex(e) + 1e-6j)
+        sig, _ = sg_mod.selfEnergy(hL=ld.hL, hLL=ld.hLL, sL=ld.sL, sLL=ld.sLL, ee=float(e),
+                                   hDL=ld.hDL, sDL=ld.sDL, etaLead=1e-6)
+        gs_all.append(gs)
+        sig_all.append(sig.numpy())
+    _put(d, "chain/energy", es)
+    _put(d, "chain/eta", np.array(1e-6))
+    for k in ("hL", "hLL", "sL", "sLL", "hDL", "sDL"):
+        _put(d, "chain/" + k, getattr(ld, k))
+    _put(d, "chain/gs", np.stack(gs_all))
+    _put(d, "chain/sigma", np.stack(sig_all))
+
+    dev = workload.random_device(6, 4, seed=7)
+    for side, ld in (("left", dev.lead_L), ("right", dev.lead_R)):
+        es = np.array([-1.7, -0.4, 0.3, 1.1])
+        gs_all, sig_all = [], []
+        for e in es:
+            sig, gs = sg_mod.selfEnergy(hL=ld.hL, hLL=ld.hLL, sL=ld.sL, sLL=ld.sLL, ee=float(e),
+                                        hDL=ld.hDL, sDL=ld.sDL, etaLead=1e-5, E_ref=0.02)
+            gs_all.append(gs.numpy())
+            sig_all.append(sig.numpy())
+        p = f"rand_{side}/"
+        _put(d, p + "energy", es)
+        _put(d, p + "eta", np.array(1e-5))
+        _put(d, p + "E_ref", np.array(0.02))
+        for k in ("hL", "hLL", "sL", "sLL", "hDL", "sDL"):
+            _put(d, p + k, getattr(ld, k))
+        _put(d, p + "gs", np.stack(gs_all))
+        _put(d, p + "sigma", np.stack(sig_all))
+    np.savez_compressed(os.path.join(HERE, "lopez_sancho.npz"), **d)
+
+
+def _ozaki_cases(oz_mod, nu_mod):
+    d = {}
+    for M in (30, 64):
+        p, r = oz_mod.ozaki_residues(M)
+        _put(d, f"M{M}/poles", p)
+        _put(d, f"M{M}/res", r)
+    xs, w = nu_mod.gauss_xw(xl=torch.scalar_tensor(-0.4, dtype=torch.float64),
+                            xu=torch.scalar_tensor(0.5, dtype=torch.float64), n=10)
+    _put(d, "gauss/x", xs)
+    _put(d, "gauss/w", w)
+    np.savez_compressed(os.path.join(HERE, "ozaki.npz"), **d)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref-root", default=ref_import.DEFAULT_REF_ROOT)
+    args = ap.parse_args()
+    torch.set_num_threads(1)  # the container's threaded batched zgesv can hang
+    rgf_mod = ref_import.load("recursive_green_cal", args.ref_root)
+    sg_mod = ref_import.load("surface_green", args.ref_root)
+    dp_mod = ref_import.load("device_property", args.ref_root)
+    oz_mod = ref_import.load("ozaki_res_cal", args.ref_root)
+    nu_mod = ref_import.load("negf_utils", args.ref_root)
+
+    _rgf_case(rgf_mod, "nonuniform_retarded", [8, 6, 8], 6, seed=1)
+    _rgf_case(rgf_mod, "uniform_retarded", [8] * 5, 6, seed=2, E_ref=0.1)
+    _rgf_case(rgf_mod, "uniform_lesser", [6] * 4, 4, seed=3, lesser=True)
+    _rgf_case(rgf_mod, "nonuniform_lesser", [5, 7, 4], 3, seed=4, lesser=True)
+    _rgf_case(rgf_mod, "scalar_retarded", [4, 4, 4], 1, seed=5, scalar=True)
+    _rgf_case(rgf_mod, "greater", [4, 5, 4], 3, seed=6, greater=True, lesser=True)
+    _rgf_case(rgf_mod, "two_blocks", [3, 3], 2, seed=8)
+    _rgf_case(rgf_mod, "wide_uniform", [20] * 4, 2, seed=9, gr_lc=False)
+    _devprop_case(dp_mod, "nonuniform", [4, 5, 4], 5, seed=10, norbs=[2, 3, 1, 3, 4])
+    _devprop_case(dp_mod, "uniform", [6] * 4, 4, seed=11, norbs=[1] * 24)
+    _lopez_cases(sg_mod)
+    _ozaki_cases(oz_mod, nu_mod)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,61 @@
+"""The C-ABI library loads on a CPU-only host and exports every declared symbol.
+
+No compute is launched here (there is no GPU); this pins the boundary: the
+entry points named in include/*.h exist, and the numpy/ctypes mirrors of the
+descriptor structs have the C sizes.
+"""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+from dpnegf_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = []
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"^\s*[A-Za-z_][\w\s\*]*?\b(negf_\w+)\s*\(", src, flags=re.M):
+            names.append(m.group(1))
+    return sorted(set(names))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "negf_rgf_run" in names and "negf_rgf_scratch_bytes" in names, names
+
+
+@pytest.mark.parametrize("name", declared_functions())
+def test_library_exports_symbol(name):
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    assert hasattr(lib, name), f"{name} declared in include/ but not exported"
+
+
+def test_struct_mirrors_match_c_sizes():
+    lib = _lib.load()
+    assert lib.negf_abi_struct_size(0) == _lib.BLOCK_DTYPE.itemsize
+    assert lib.negf_abi_struct_size(1) == _lib.DEVICE_DTYPE.itemsize
+    assert lib.negf_abi_struct_size(2) == _lib.ITEM_DTYPE.itemsize
+    assert lib.negf_abi_struct_size(3) == ctypes.sizeof(_lib.NegfRgfProblem)
+
+
+def test_scratch_query_without_gpu():
+    lib = _lib.load()
+    p = _lib.NegfRgfProblem()
+    p.n_slots, p.max_n, p.max_g_slab, p.flags = 2, 64, 64 * 64 * 3, 0
+    need = lib.negf_rgf_scratch_bytes(ctypes.byref(p))
+    assert need >= 2 * (18 * 64 * 64 + 64 * 64 * 3) * 16
+    p.flags = _lib.OUT_GR_LEFT
+    assert lib.negf_rgf_scratch_bytes(ctypes.byref(p)) < need
+
+
+def test_run_rejects_bad_arguments_without_launch():
+    lib = _lib.load()
+    p = _lib.NegfRgfProblem()
+    assert lib.negf_rgf_run(ctypes.byref(p), None) == _lib.NEGF_ERR_ARGUMENT

@@ -1,0 +1,112 @@
+"""The numpy oracle reproduces the reference's own outputs (CPU only).
+
+The fixtures were produced by the reference implementation itself
+(``tests/golden/make_golden.py``); this pins the oracle before it is used to
+check the CUDA path.
+"""
+import numpy as np
+import pytest
+
+from oracle import lead_oracle, rgf_oracle
+from tests.goldens import Golden, rgf_cases
+
+TAGS = rgf_oracle.TAGS
+
+
+def _close(a, b, atol=1e-10, rtol=1e-10):
+    a, b = np.asarray(a), np.asarray(b)
+    assert a.shape == b.shape, (a.shape, b.shape)
+    np.testing.assert_allclose(a, b, atol=atol, rtol=rtol)
+
+
+def run_oracle_on(g):
+    scalar = bool(g["scalar"])
+    kw = dict(eta=float(g["eta"]), E_ref=float(g["E_ref"]),
+              need_lesser=g.has("s_in"), need_greater=g.has("s_out"),
+              need_gr_lc=g.has("out/gr_lc"))
+    return rgf_oracle.rgf(g["energy"], g["hl"], g["hd"], g["hu"], g["sd"], g["su"], g["sl"],
+                          g["left_se"], g["right_se"], s_in=g.get("s_in"), s_out=g.get("s_out"), **kw)
+
+
+@pytest.mark.parametrize("case", rgf_cases())
+def test_rgf_oracle_matches_reference(case):
+    g = Golden(case)
+    out = run_oracle_on(g)
+    scalar = bool(g["scalar"])
+    for t in TAGS:
+        key = "out/" + t
+        if not g.has(key):
+            assert out[t] is None or t == "gr_lc" or t == "gr_left", t
+            continue
+        ref = g[key]
+        mine = out[t]
+        if isinstance(ref, list):
+            assert len(ref) == len(mine), t
+            for r, m in zip(ref, mine):
+                _close(m[0] if scalar else m, r)
+        else:
+            _close(mine[0] if scalar else mine, ref)
+
+
+@pytest.mark.parametrize("case", ["devprop_nonuniform", "devprop_uniform"])
+def test_device_traces_match_reference(case):
+    g = Golden(case)
+    E = g["energy"]
+    Eref = float(g["E_ref"])
+    dims = list(g["dims"])
+    kBT = float(g["kBT"])
+    sinL_f = rgf_oracle.fermi_dirac(np.real(E) + Eref, float(g["muL"]), kBT)
+    sinR_f = rgf_oracle.fermi_dirac(np.real(E) + Eref, float(g["muR"]), kBT)
+    s_in = rgf_oracle.s_in_from_se(g["left_se"], g["right_se"], sinL_f, sinR_f, dims)
+    out = rgf_oracle.rgf(E, g["hl"], g["hd"], g["hu"], g["sd"], g["su"], g["sl"],
+                         g["left_se"], g["right_se"], E_ref=Eref, eta=float(g["eta_device"]),
+                         s_in=s_in, need_lesser=True)
+    tc = rgf_oracle.transmission(out["g_trans"], rgf_oracle.gamma_from_se(g["left_se"]),
+                                 rgf_oracle.gamma_from_se(g["right_se"]))
+    _close(tc, g["out/tc"])
+    d = rgf_oracle.dos(out["grd"], out["grl"], out["gru"], g["sd"], g["su"], g["sl"])
+    _close(d, g["out/dos"])
+    ld = rgf_oracle.ldos(out["grd"], out["grl"], out["gru"], g["sd"], g["su"], g["sl"], list(g["norbs"]))
+    _close(ld, g["out/ldos"])
+    for r, m in zip(g["out/gnd"], out["gnd"]):
+        _close(m, r)
+
+
+@pytest.mark.parametrize("lead", ["chain", "rand_left", "rand_right"])
+def test_lopez_sancho_oracle_matches_reference(lead):
+    g = Golden("lopez_sancho")
+    p = lead + "/"
+    Eref = float(g[p + "E_ref"]) if g.has(p + "E_ref") else 0.0
+    eta = float(g[p + "eta"])
+    for i, e in enumerate(g[p + "energy"]):
+        sig, gs, st, it = lead_oracle.self_energy(g[p + "hL"], g[p + "hLL"], g[p + "sL"], g[p + "sLL"], e,
+                                                  g[p + "hDL"], g[p + "sDL"], etaLead=eta, E_ref=Eref)
+        assert st in (lead_oracle.LS_OK, lead_oracle.LS_WARN)
+        _close(gs, g[p + "gs"][i], atol=1e-9, rtol=1e-8)
+        _close(sig, g[p + "sigma"][i], atol=1e-9, rtol=1e-8)
+
+
+def test_chain_surface_green_is_analytic():
+    """1-D chain (t=-1): the lead self-energy is t^2 g_s with g_s the closed form."""
+    g = Golden("lopez_sancho")
+    for i, e in enumerate(g["chain/energy"]):
+        z = complex(e) + 1j * float(g["chain/eta"])
+        # surface site Green function of a semi-infinite chain with hopping t=-1
+        root = np.sqrt(z * z - 4.0 + 0j)
+        gs1 = (z - root) / 2.0
+        if gs1.imag > 0:
+            gs1 = (z + root) / 2.0
+        sig = g["chain/sigma"][i]
+        # the single coupled site of the last device block carries t^2 g_s
+        assert abs(sig[1, 1] - gs1) < 1e-5, (e, sig[1, 1], gs1)
+
+
+def test_ozaki_and_gauss_match_reference():
+    g = Golden("ozaki")
+    for M in (30, 64):
+        p, r = lead_oracle.ozaki_residues(M)
+        _close(p, g[f"M{M}/poles"], atol=0, rtol=1e-12)
+        _close(r, g[f"M{M}/res"], atol=0, rtol=1e-10)
+    x, w = lead_oracle.gauss_xw(-0.4, 0.5, 10)
+    _close(x, g["gauss/x"], atol=1e-15, rtol=0)
+    _close(w, g["gauss/w"], atol=1e-15, rtol=0)

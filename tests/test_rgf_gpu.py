@@ -1,0 +1,150 @@
+"""RGF parity on the GPU: the CUDA sweep against the reference fixtures and
+the numpy oracle.  Tolerance: FP64 path within 1e-10 relative (max-norm of
+each block), as required for the plain path."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import lead_oracle, rgf_oracle
+from tests.goldens import Golden, rgf_cases
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-10
+
+
+def _cu(xs):
+    return [torch.as_tensor(x).cuda() for x in xs]
+
+
+def _assert_block_close(got, want, tag, rtol=RTOL):
+    got = got.detach().cpu().numpy() if torch.is_tensor(got) else np.asarray(got)
+    want = np.asarray(want)
+    assert got.shape == want.shape, (tag, got.shape, want.shape)
+    scale = max(np.abs(want).max(), 1e-300)
+    err = np.abs(got - want).max() / scale
+    assert err < rtol, f"{tag}: relative max error {err:.3e}"
+
+
+def _compare(ans, ref_get, scalar=False):
+    for i, tag in enumerate(rgf_oracle.TAGS):
+        want = ref_get(tag)
+        got = ans[i]
+        if want is None:
+            continue
+        assert got is not None, tag
+        if isinstance(want, list):
+            assert len(got) == len(want), tag
+            for q, (g, w) in enumerate(zip(got, want)):
+                _assert_block_close(g, w, f"{tag}[{q}]")
+        else:
+            _assert_block_close(got, want, tag)
+
+
+@pytest.mark.parametrize("case", rgf_cases())
+def test_rgf_matches_reference_fixture(case):
+    from dpnegf_b200.recursive_green_cal import recursive_gf
+    g = Golden(case)
+    scalar = bool(g["scalar"])
+    E = torch.as_tensor(g["energy"]).cuda()
+    seL, seR = torch.as_tensor(g["left_se"]).cuda(), torch.as_tensor(g["right_se"]).cuda()
+    lesser = g.has("s_in")
+    kw = dict(eta=float(g["eta"]), E_ref=float(g["E_ref"]), need_gr_lc=g.has("out/gr_lc"))
+    if g.has("s_out"):
+        pytest.skip("G^> sweep is not provided")
+    if scalar:
+        ans = recursive_gf(E[0], _cu(g["hl"]), _cu(g["hd"]), _cu(g["hu"]), _cu(g["sd"]), _cu(g["su"]),
+                           _cu(g["sl"]), seL[0], seR[0],
+                           s_in=[torch.as_tensor(s[0]).cuda() for s in g["s_in"]] if lesser else 0,
+                           need_lesser=lesser, **kw)
+    else:
+        ans = recursive_gf(E, _cu(g["hl"]), _cu(g["hd"]), _cu(g["hu"]), _cu(g["sd"]), _cu(g["su"]),
+                           _cu(g["sl"]), seL, seR, s_in=_cu(g["s_in"]) if lesser else 0,
+                           need_lesser=lesser, **kw)
+    _compare(ans, lambda t: g.get("out/" + t))
+
+
+def _oracle_case(dims, B, seed, lesser=False, eta=1e-5):
+    from dpnegf_b200 import workload
+    dev = workload.random_device(0, 0, seed=seed, block_dims=dims)
+    seL = workload.random_self_energy(B, dims[0], seed=seed + 1)
+    seR = workload.random_self_energy(B, dims[-1], seed=seed + 2)
+    E = torch.linspace(-2.0, 2.0, B, dtype=torch.float64).to(torch.complex128)
+    s_in = None
+    if lesser:
+        f = np.linspace(0.1, 0.9, B)
+        s_in = rgf_oracle.s_in_from_se(seL.numpy(), seR.numpy(), f, 1 - f, dims)
+    return dev, seL, seR, E, s_in
+
+
+@pytest.mark.parametrize("dims,B", [([64] * 4, 3), ([70, 33, 128, 65], 2), ([256] * 3, 2),
+                                     ([300, 280], 1), ([17], 3), ([96, 96], 5)])
+def test_rgf_matches_oracle_sizes(dims, B):
+    """Ragged tiles (n not a multiple of 64), the NB=16 inverse (n>256), K=1, K=2."""
+    from dpnegf_b200.recursive_green_cal import recursive_gf
+    dev, seL, seR, E, _ = _oracle_case(dims, B, seed=len(dims) * 7 + dims[0])
+    ans = recursive_gf(E.cuda(), _cu(dev.hl), _cu(dev.hd), _cu(dev.hu), _cu(dev.sd), _cu(dev.su),
+                       _cu(dev.sl), seL.cuda(), seR.cuda(), eta=1e-5, need_gr_lc=True)
+    ref = rgf_oracle.rgf(E.numpy(), [x.numpy() for x in dev.hl], [x.numpy() for x in dev.hd],
+                         [x.numpy() for x in dev.hu], [x.numpy() for x in dev.sd],
+                         [x.numpy() for x in dev.su], [x.numpy() for x in dev.sl],
+                         seL.numpy(), seR.numpy(), eta=1e-5, need_gr_lc=True)
+    _compare(ans, lambda t: ref.get(t))
+
+
+def test_rgf_lesser_matches_oracle():
+    from dpnegf_b200.recursive_green_cal import recursive_gf
+    dims = [40, 72, 40]
+    dev, seL, seR, E, s_in = _oracle_case(dims, 3, seed=11, lesser=True)
+    ans = recursive_gf(E.cuda(), _cu(dev.hl), _cu(dev.hd), _cu(dev.hu), _cu(dev.sd), _cu(dev.su),
+                       _cu(dev.sl), seL.cuda(), seR.cuda(), eta=1e-5, need_lesser=True,
+                       s_in=[torch.as_tensor(s).cuda() for s in s_in])
+    ref = rgf_oracle.rgf(E.numpy(), [x.numpy() for x in dev.hl], [x.numpy() for x in dev.hd],
+                         [x.numpy() for x in dev.hu], [x.numpy() for x in dev.sd],
+                         [x.numpy() for x in dev.su], [x.numpy() for x in dev.sl],
+                         seL.numpy(), seR.numpy(), eta=1e-5, s_in=s_in, need_lesser=True)
+    _compare(ans, lambda t: ref.get(t))
+
+
+@pytest.mark.parametrize("dims", [[8, 6, 8], [128] * 5, [256] * 4])
+def test_fused_transmission_and_dos(dims):
+    """T(E) and per-orbital DOS reduced inside the sweep vs the oracle."""
+    from dpnegf_b200 import rgf_plan
+    B = 4
+    dev, seL, seR, E, _ = _oracle_case(dims, B, seed=5)
+    geom = rgf_plan.Geometry([rgf_plan.DeviceBlocks(dev.hd, dev.hu, dev.hl, dev.sd, dev.su, dev.sl)])
+    res = rgf_plan.run(geom, [E.cuda()], [seL.cuda()], [seR.cuda()], eta=1e-5, outputs=(),
+                       trans=True, orb_dos=True)
+    ref = rgf_oracle.rgf(E.numpy(), [x.numpy() for x in dev.hl], [x.numpy() for x in dev.hd],
+                         [x.numpy() for x in dev.hu], [x.numpy() for x in dev.sd],
+                         [x.numpy() for x in dev.su], [x.numpy() for x in dev.sl],
+                         seL.numpy(), seR.numpy(), eta=1e-5)
+    T = rgf_oracle.transmission(ref["g_trans"], rgf_oracle.gamma_from_se(seL.numpy()),
+                                rgf_oracle.gamma_from_se(seR.numpy()))
+    dos = rgf_oracle.dos(ref["grd"], ref["grl"], ref["gru"], [x.numpy() for x in dev.sd],
+                         [x.numpy() for x in dev.su], [x.numpy() for x in dev.sl])
+    got_T = res.trans.cpu().numpy()
+    got_dos = 2.0 * res.orb_dos.cpu().numpy().reshape(B, -1).sum(-1)
+    np.testing.assert_allclose(got_T, T, rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(got_dos, dos, rtol=1e-10, atol=1e-12)
+
+
+def test_chain_transmission_is_one_in_band():
+    """1-D chain, t=-1, leads from the oracle decimation: T(E)=1 for |E|<1.9."""
+    from dpnegf_b200 import rgf_plan, workload
+    chain = workload.chain_device(L=10)
+    E = np.linspace(-3, 3, 61)
+    seL, seR = [], []
+    for e in E:
+        for side, acc in ((chain.lead_L, seL), (chain.lead_R, seR)):
+            s, _, st, _ = lead_oracle.self_energy(side.hL.numpy(), side.hLL.numpy(), side.sL.numpy(),
+                                                  side.sLL.numpy(), e, side.hDL.numpy(), side.sDL.numpy(),
+                                                  etaLead=1e-6)
+            acc.append(s)
+    geom = rgf_plan.Geometry([rgf_plan.DeviceBlocks(chain.hd, chain.hu, chain.hl, chain.sd, chain.su, chain.sl)])
+    res = rgf_plan.run(geom, [torch.as_tensor(E).to(torch.complex128).cuda()],
+                       [torch.as_tensor(np.stack(seL)).cuda()], [torch.as_tensor(np.stack(seR)).cuda()],
+                       eta=1e-6, outputs=(), trans=True, orb_dos=True)
+    T = res.trans.cpu().numpy()
+    inband = np.abs(E) < 1.9
+    assert np.all(np.abs(T[inband] - 1.0) < 1e-4), T[inband]
+    assert np.all(T[np.abs(E) > 2.1] < 1e-8)

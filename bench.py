@@ -1,0 +1,330 @@
+#!/usr/bin/env python
+"""Benchmark: batched FP64 RGF energy-points/s at b=256, L=64 on B200.
+
+Workload (synthetic, seeded): random Hermitian tight-binding device with
+block size b=256 and L=64 blocks (onsite diag U[-2,2] eV + Hermitian Gaussian
+sigma=0.3/sqrt(b); couplings Gaussian sigma=1/sqrt(b); S = I + Hermitian
+Gaussian sigma=0.01/sqrt(b), non-zero S couplings), 2048 energies in [-3,3] eV,
+eta=1e-5, complex128.  One step = one k-realisation (its own seeded device)
+over all 2048 energies: the full RGF sweep with T(E) and DOS reduced in the
+same launch.  Each rank handles its own k-realisations (weak scaling, no
+data-path collective).
+
+Prints one JSON line (rank 0).  ``--impl reference`` times the CPU oracle
+(numpy restatement of the reference recursive_gf + T/DOS) on the host cores
+for the same workload instead.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RGF energy-points/s @ b=256,L=64: FP64 vs mixed+adjoint on 1 B200; % roofline"
+UNIT = "energy-points/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--b", type=int, default=256)
+    ap.add_argument("--L", type=int, default=64)
+    ap.add_argument("--energies", type=int, default=2048)
+    ap.add_argument("--eta", type=float, default=1e-5)
+    ap.add_argument("--cpu-energies", type=int, default=0, help="CPU baseline sample size (0: one per process)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--phases", action="store_true", help="report per-phase SM-cycle shares")
+    return ap.parse_args()
+
+
+def flops_per_point(b, L):
+    """Algorithmic work of one retarded RGF energy point: 9 complex n^3 MACs per block (4M)."""
+    return 72.0 * b ** 3 * L
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_fp64_peak(torch):
+    """cuBLAS DGEMM (FP64 tensor cores) 8192^3, best of 5 -- the FP64 roofline denominator."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    c = a @ b
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.mm(a, b, out=c)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def traffic_per_point(b, L):
+    """DRAM bytes per energy point from the committed ncu summary, scaled by block count."""
+    path = os.path.join(ROOT, "profiles", "rgf_kernel_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        if int(d["b"]) == b:
+            return float(d["dram_bytes_per_point_per_block"]) * L
+    except Exception:
+        pass
+    return None
+
+
+def cpu_procs():
+    n = os.cpu_count() or 1
+    try:
+        import psutil
+        mem_gb = psutil.virtual_memory().available / 2 ** 30
+        n = min(n, max(1, int(mem_gb // 1.5)))
+    except Exception:
+        pass
+    return max(1, min(n, 64))
+
+
+def cpu_baseline(args, seed, target_seconds=20.0):
+    """Oracle RGF on host cores over a bounded sample of the workload's energies."""
+    import numpy as np
+    from oracle import cpu_baseline as cb
+    procs = cpu_procs()
+    nE = args.cpu_energies or procs
+    E = np.linspace(-3.0, 3.0, args.energies)[:: max(1, args.energies // nE)][:nE]
+    seL, seR = cb._self_energies(args.b, len(E), seed)
+    T, D, wall = cb.run_sample(args.b, args.L, seed, E, seL, seR, args.eta, procs)
+    return {"value": len(E) / wall, "unit": UNIT, "cores": procs, "kind": "port",
+            "sample": f"{len(E)} energies of the b={args.b} L={args.L} workload (k-seed {seed}), "
+                      f"numpy oracle RGF + T/DOS, {procs} spawn processes x 1 BLAS thread, {wall:.1f} s"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    vals = []
+    base = None
+    for s in range(args.warmup + args.steps):
+        base = cpu_baseline(args, seed=1000 + s)
+        if s >= args.warmup:
+            vals.append(base["value"])
+    v = statistics.median(vals) if vals else base["value"]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": f"random Hermitian TB device b={args.b} L={args.L}, energies in [-3,3] eV, "
+                                   f"eta={args.eta}, T(E)+DOS", "b": args.b, "L": args.L},
+            "cpu_baseline": dict(base, value=v),
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    # the CPU baseline pool is spawned before any CUDA work
+    cpu_line = None
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu_line = cpu_baseline(args, seed=0)
+
+    import torch
+    import torch.distributed as dist
+    from dpnegf_b200 import _lib, rgf_plan, transport, workload
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    _lib.load()
+
+    b, L, B = args.b, args.L, args.energies
+    E = torch.linspace(-3.0, 3.0, B, dtype=torch.float64).to(torch.complex128)
+    seL_h = workload.random_self_energy(B, b, seed=1)
+    seR_h = workload.random_self_energy(B, b, seed=2)
+    seL, seR = seL_h.cuda(), seR_h.cuda()
+    Ed = E.cuda()
+    nsteps = args.warmup + args.steps
+    devs = [workload.random_device(b, L, seed=rank + world * s) for s in range(nsteps)]
+    geoms = [rgf_plan.Geometry([rgf_plan.DeviceBlocks(d.hd, d.hu, d.hl, d.sd, d.su, d.sl)]) for d in devs]
+    torch.cuda.synchronize()
+
+    peak = measured_fp64_peak(torch)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def step(s, ev=None, phase=False):
+        return rgf_plan.run(geoms[s], [Ed], [seL], [seR], eta=args.eta, outputs=(), trans=True, dos=True,
+                            check=False, events=ev, phase=phase)
+
+    for s in range(args.warmup):
+        r = step(s)
+    torch.cuda.synchronize()
+    st = r.status.cpu()
+    assert int((st != 0).sum()) == 0, "warm-up produced failing items"
+
+    clocks = Clocks(torch.cuda.current_device())
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for i in range(args.steps):
+        step(args.warmup + i, ev=kev[i])
+    t1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = t0.elapsed_time(t1)
+    kms = [a.elapsed_time(b_) for a, b_ in kev]
+    if world > 1:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = world * B * args.steps / (ms * 1e-3)
+
+    # roofline of the dominant kernel (rgf_kernel): algorithmic flops per launch / launch time
+    k_avg = sum(kms) / len(kms)
+    achieved = flops_per_point(b, L) * B / (k_avg * 1e-3) / 1e12
+    tpp = traffic_per_point(b, L)
+    roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "traffic": tpp * B if tpp else None, "kernel": "negf::rgf_kernel",
+            "algorithmic": f"72*b^3*L flop/energy point (9 complex n^3 MACs per block, 4M count; "
+                           f"3M products not credited) x {B} points per launch",
+            "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run (of measured; "
+                           "MEASURED_PEAKS.json has no FP64 figure)"}
+
+    phases = None
+    if args.phases:
+        r = step(args.warmup, phase=True)
+        torch.cuda.synchronize()
+        pc = r.phase_cycles.sum(0).double()
+        phases = {n: float(v) for n, v in zip(_lib.PHASES, (pc / pc.sum()).tolist())}
+
+    # end-to-end through the public API: pinned host inputs, host outputs
+    e2e = None
+    if not args.no_e2e:
+        d = devs[args.warmup]
+        pin = lambda xs: [x.contiguous().pin_memory() for x in xs]
+        hd, hu, hl, sd, su, sl = pin(d.hd), pin(d.hu), pin(d.hl), pin(d.sd), pin(d.su), pin(d.sl)
+        Eh, sLh, sRh = E.pin_memory(), seL_h.pin_memory(), seR_h.pin_memory()
+        h2d = sum(x.numel() * 16 for x in hd + hu + hl + sd + su + sl) + (sLh.numel() + sRh.numel() + Eh.numel()) * 16
+        d2h = 2 * B * 8
+        transport.transmission_dos(hd, hu, hl, sd, su, sl, Eh, sLh, sRh, eta=args.eta)  # warm
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        n_e2e = 1
+        for _ in range(n_e2e):
+            T, D, _ = transport.transmission_dos(hd, hu, hl, sd, su, sl, Eh, sLh, sRh, eta=args.eta)
+        e1.record()
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1)
+        if world > 1:
+            tt = torch.tensor([ems], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ems = float(tt.item())
+        e2e = {"value": world * B * n_e2e / (ems * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h,
+               "path": "dpnegf_b200.transport.transmission_dos with pinned host H/S blocks, self-energies "
+                       "and energies; T(E) and DOS returned to host"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+                "path": "fp64",
+                "config": {"workload": f"random Hermitian TB device b={b} L={L}, {B} energies in [-3,3] eV per "
+                                       f"k-realisation (step), eta={args.eta}, complex128, T(E)+DOS fused",
+                           "b": b, "L": L, "energies_per_step": B, "k_per_step_per_gpu": 1,
+                           "l2": "inputs larger than L2 (H/S arena 380 MiB per step, per-slot scratch 82 MiB x 148)",
+                           "parallelism": f"k-realisations across {world} GPU(s)"},
+                "roofline": roof, "cpu_baseline": cpu_line, "e2e": e2e, "clocks": clk,
+                "gpu_launches": args.steps, "kernel_ms": kms}
+        if phases:
+            line["phases"] = phases
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

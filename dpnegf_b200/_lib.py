@@ -34,6 +34,8 @@ OUT_GR_LEFT = 1 << 5
 TRANS = 1 << 6
 ORB_DOS = 1 << 7
 LESSER = 1 << 8
+DOS = 1 << 9
+PHASES = ("form", "gemm_fwd", "inverse", "gemm_bwd", "lesser", "dos", "trans", "other")
 
 # numpy mirrors of the descriptor structs (packed exactly like the C structs)
 BLOCK_FIELDS = ["hd", "sd", "hu", "su", "hl", "sl", "orb0", "g", "o_grd", "o_grl", "o_gru", "o_grlc",
@@ -42,7 +44,7 @@ BLOCK_DTYPE = np.dtype([("n", "<i4"), ("n_next", "<i4")] + [(f, "<i8") for f in 
 DEVICE_DTYPE = np.dtype([("n_blocks", "<i4"), ("blk0", "<i4"), ("n_orb", "<i4"), ("pad", "<i4"),
                          ("o_gtrans", "<i8"), ("g_slab", "<i8")])
 ITEM_DTYPE = np.dtype([("dev", "<i4"), ("row", "<i4"), ("z_re", "<f8"), ("z_im", "<f8"),
-                       ("se_l", "<i8"), ("se_r", "<i8"), ("nse_l", "<i4"), ("nse_r", "<i4"),
+                       ("se_l", "<u8"), ("se_r", "<u8"), ("nse_l", "<i4"), ("nse_r", "<i4"),
                        ("out", "<i8"), ("orb", "<i8")])
 
 
@@ -55,16 +57,17 @@ class NegfRgfProblem(ctypes.Structure):
         ("max_n", ctypes.c_int32),
         ("max_g_slab", ctypes.c_int64),
         ("hs", ctypes.c_void_p),
-        ("se", ctypes.c_void_p),
         ("s_in", ctypes.c_void_p),
         ("out", ctypes.c_void_p),
         ("trans", ctypes.c_void_p),
         ("orb_dos", ctypes.c_void_p),
+        ("dos", ctypes.c_void_p),
         ("status", ctypes.c_void_p),
         ("flags", ctypes.c_uint32),
         ("n_slots", ctypes.c_int32),
         ("scratch", ctypes.c_void_p),
         ("scratch_bytes", ctypes.c_size_t),
+        ("phase_cycles", ctypes.c_void_p),
     ]
 
 

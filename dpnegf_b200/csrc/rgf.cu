@@ -94,8 +94,10 @@ NEGF_DEV void copy_mat(cplx* dst, const cplx* src, int m, int n) {
   for (int e = threadIdx.x; e < m * n; e += CTA_THREADS) dst[e] = src[e];
 }
 
-// dst[i] (+)= -Im( sum_j A[i][j] B[j][i] ) / pi   (A: rows x inner, B: inner x rows)
-NEGF_DEV void diag_im_acc(double* dst, const cplx* A, const cplx* B, int rows, int inner, bool init) {
+// dst[i] (+)= -Im( sum_j A[i][j] B[j][i] ) / pi   (A: rows x inner, B: inner x rows).
+// dst may be null; the row values are also summed into dsum (lane 0 of each warp).
+NEGF_DEV void diag_im_acc(double* dst, double& dsum, const cplx* A, const cplx* B, int rows, int inner,
+                          bool init) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int i = warp; i < rows; i += CTA_THREADS / 32) {
     double acc = 0.0;
@@ -107,10 +109,32 @@ NEGF_DEV void diag_im_acc(double* dst, const cplx* A, const cplx* B, int rows, i
     for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
     if (lane == 0) {
       double v = -acc * 0.31830988618379067154;  // 1/pi
-      dst[i] = init ? v : dst[i] + v;
+      dsum += v;
+      if (dst) dst[i] = init ? v : dst[i] + v;
     }
   }
 }
+
+// Per-CTA phase clocks (thread 0): the cycles since the previous mark are
+// charged to the phase that just ended.  Every mark follows a __syncthreads.
+enum Phase { PH_FORM = 0, PH_GEMM_FWD, PH_INV, PH_GEMM_BWD, PH_LESSER, PH_DOS, PH_TRANS, PH_OTHER, NPH };
+struct PhaseClock {
+  unsigned long long c[NPH];
+  long long t0;
+  bool on;
+  NEGF_DEV void start(bool enable) {
+    on = enable && threadIdx.x == 0;
+    for (int i = 0; i < NPH; ++i) c[i] = 0;
+    t0 = on ? clock64() : 0;
+  }
+  NEGF_DEV void mark(int ph) {
+    if (on) {
+      long long t = clock64();
+      c[ph] += (unsigned long long)(t - t0);
+      t0 = t;
+    }
+  }
+};
 
 // Gamma = i (Sigma - Sigma^H) on the c x c corner of Sigma (ns x ns) at (r0, r0).
 NEGF_DEV void form_gamma(cplx* out, const cplx* se, int ns, int r0, int c) {
@@ -146,7 +170,7 @@ NEGF_DEV void gemm(cplx* smem, int M, int N, int K, const cplx* A, int64_t lda, 
 }
 
 NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBufs& sb, char* smem_raw,
-                       double* red) {
+                       double* red, PhaseClock& pc) {
   cplx* smem = reinterpret_cast<cplx*>(smem_raw);
   const NegfDevice dv = P.devices[it.dev];
   const NegfBlock* blk = P.blocks + dv.blk0;
@@ -155,11 +179,10 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
   const uint32_t fl = P.flags;
   const cplx z = cmk(it.z_re, it.z_im);
   const cplx* hs = reinterpret_cast<const cplx*>(P.hs);
-  const cplx* se = reinterpret_cast<const cplx*>(P.se);
   const cplx* sin = reinterpret_cast<const cplx*>(P.s_in);
   cplx* out = reinterpret_cast<cplx*>(P.out);
-  const cplx* seL = it.se_l >= 0 ? se + it.se_l : nullptr;
-  const cplx* seR = it.se_r >= 0 ? se + it.se_r : nullptr;
+  const cplx* seL = reinterpret_cast<const cplx*>(it.se_l);
+  const cplx* seR = reinterpret_cast<const cplx*>(it.se_r);
   const cplx ONE = cmk(1.0, 0.0), MONE = cmk(-1.0, 0.0);
   const bool lesser = (fl & NEGF_LESSER) != 0;
   int bad = 0;
@@ -186,12 +209,16 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
       form_shift(sb.Lz, hs, bp.hl, bp.sl, z, nq, np);  // L_{q-1}: n_q x n_{q-1}
       form_shift(sb.Uz, hs, bp.hu, bp.su, z, np, nq);  // U_{q-1}: n_{q-1} x n_q
       __syncthreads();
+      pc.mark(PH_FORM);
       gemm<OP_N, OP_N>(smem, nq, np, np, sb.Lz, np, gptr(q - 1), np, sb.T1, np);
       gemm<OP_N, OP_N>(smem, nq, nq, np, sb.T1, np, sb.Uz, nq, sb.W, nq, MONE, sb.W, nq);
+      pc.mark(PH_GEMM_FWD);
     } else {
       __syncthreads();
+      pc.mark(PH_FORM);
     }
     bad |= cta_inverse(sb.W, nq, nq, gptr(q), nq, smem_raw);
+    pc.mark(PH_INV);
     if (lesser) {
       // gin_q = g_q (s_q + L gin_{q-1} U) g_q^H
       const cplx* s = sinptr(q);
@@ -207,13 +234,16 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
       }
       gemm<OP_N, OP_N>(smem, nq, nq, nq, gptr(q), nq, sb.tA, nq, sb.tB, nq);
       gemm<OP_N, OP_C>(smem, nq, nq, nq, sb.tB, nq, gptr(q), nq, ginptr(q), nq);
+      pc.mark(PH_LESSER);
     }
   }
 
   // ----------------------------------------------------------- backward sweep
   const int nN = blk[K - 1].n;
   const bool need_gt = (fl & (NEGF_OUT_GTRANS | NEGF_OUT_GR_LC | NEGF_TRANS)) != 0;
+  const bool want_dos = (fl & (NEGF_ORB_DOS | NEGF_DOS)) != 0;
   double* orb = (fl & NEGF_ORB_DOS) ? P.orb_dos + it.orb : nullptr;
+  double dsum = 0.0;  // per-thread partial of sum_i -Im diag(GS)_i / pi
 
   const cplx* Gnext = gptr(K - 1);
   if (fl & NEGF_OUT_GRD) {
@@ -237,9 +267,11 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
     }
   }
   __syncthreads();
-  if (orb) {
-    diag_im_acc(orb + blk[K - 1].orb0, gptr(K - 1), hs + blk[K - 1].sd, nN, nN, true);
+  pc.mark(PH_FORM);
+  if (want_dos) {
+    diag_im_acc(orb ? orb + blk[K - 1].orb0 : nullptr, dsum, gptr(K - 1), hs + blk[K - 1].sd, nN, nN, true);
     __syncthreads();
+    pc.mark(PH_DOS);
   }
   int tog = 0;
   for (int q = K - 2; q >= 0; --q) {
@@ -249,6 +281,7 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
     form_shift(sb.Lz, hs, b.hl, b.sl, z, nn, nq);  // L_q: n_{q+1} x n_q
     form_shift(sb.Uz, hs, b.hu, b.su, z, nq, nn);  // U_q: n_q x n_{q+1}
     __syncthreads();
+    pc.mark(PH_FORM);
     const cplx* g = gptr(q);
     cplx* grl = (fl & NEGF_OUT_GRL) ? out + b.o_grl + row * szu : sb.Gl;
     cplx* gru = (fl & NEGF_OUT_GRU) ? out + b.o_gru + row * szu : sb.Gu;
@@ -264,6 +297,7 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
       gt = gtn;
       tog ^= 1;
     }
+    pc.mark(PH_GEMM_BWD);
     if (lesser) {
       const cplx* gin = ginptr(q);
       cplx* gnl = b.o_gnl >= 0 ? out + b.o_gnl + row * szu : sb.Nl;
@@ -288,12 +322,20 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
       }
       __syncthreads();
       Nnext = gnd;
+      pc.mark(PH_LESSER);
     }
-    if (orb) {
-      diag_im_acc(orb + b.orb0, grd, hs + b.sd, nq, nq, true);
+    if (want_dos) {
+      diag_im_acc(orb ? orb + b.orb0 : nullptr, dsum, grd, hs + b.sd, nq, nq, true);
       __syncthreads();
-      if (b.sl >= 0) { diag_im_acc(orb + b.orb0, gru, hs + b.sl, nq, nn, false); __syncthreads(); }
-      if (b.su >= 0) { diag_im_acc(orb + blk[q + 1].orb0, grl, hs + b.su, nn, nq, false); __syncthreads(); }
+      if (b.sl >= 0) {
+        diag_im_acc(orb ? orb + b.orb0 : nullptr, dsum, gru, hs + b.sl, nq, nn, false);
+        __syncthreads();
+      }
+      if (b.su >= 0) {
+        diag_im_acc(orb ? orb + blk[q + 1].orb0 : nullptr, dsum, grl, hs + b.su, nn, nq, false);
+        __syncthreads();
+      }
+      pc.mark(PH_DOS);
     }
     Gnext = grd;
   }
@@ -302,6 +344,9 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
     copy_mat(d, gt, blk[0].n, nN);
     __syncthreads();
   }
+  double dos_total = 0.0;
+  if (fl & NEGF_DOS) dos_total = 2.0 * cta_sum(dsum, red);
+  pc.mark(PH_DOS);
 
   // ------------------------------------------------------------ T(E)
   double tval = 0.0;
@@ -324,12 +369,14 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
   }
   if (threadIdx.x == 0) {
     if (fl & NEGF_TRANS) P.trans[it.out] = tval;
+    if (fl & NEGF_DOS) P.dos[it.out] = dos_total;
     int st = NEGF_OK;
     if (bad) st = NEGF_ERR_SINGULAR;
-    else if (!isfinite(tval)) st = NEGF_ERR_NONFINITE;
+    else if (!isfinite(tval) || !isfinite(dos_total)) st = NEGF_ERR_NONFINITE;
     P.status[it.out] = st;
   }
   __syncthreads();
+  pc.mark(PH_TRANS);
 }
 
 __global__ void __launch_bounds__(CTA_THREADS, 1) rgf_kernel(const NegfRgfProblem P) {
@@ -338,15 +385,20 @@ __global__ void __launch_bounds__(CTA_THREADS, 1) rgf_kernel(const NegfRgfProble
   __shared__ double red[CTA_THREADS / 32];
   unsigned* queue = reinterpret_cast<unsigned*>(P.scratch);
   const SlotBufs sb = slot_bufs(P, blockIdx.x);
+  PhaseClock pc;
+  pc.start(P.phase_cycles != nullptr);
   for (;;) {
     if (threadIdx.x == 0) s_item = (int)atomicAdd(queue, 1u);
     __syncthreads();
     const int idx = s_item;
     __syncthreads();
+    pc.mark(PH_OTHER);
     if (idx >= P.n_items) break;
     const NegfItem it = P.items[idx];
-    rgf_item(P, it, sb, smem, red);
+    rgf_item(P, it, sb, smem, red, pc);
   }
+  if (pc.on)
+    for (int i = 0; i < NPH; ++i) P.phase_cycles[(size_t)blockIdx.x * NPH + i] = pc.c[i];
 }
 
 size_t rgf_smem_bytes(int max_n) {
@@ -372,6 +424,7 @@ int negf_rgf_run(const NegfRgfProblem* p, void* stream) {
   if ((reinterpret_cast<uintptr_t>(p->scratch) & 255) != 0) return NEGF_ERR_ARGUMENT;
   if ((p->flags & NEGF_TRANS) && !p->trans) return NEGF_ERR_ARGUMENT;
   if ((p->flags & NEGF_ORB_DOS) && !p->orb_dos) return NEGF_ERR_ARGUMENT;
+  if ((p->flags & NEGF_DOS) && !p->dos) return NEGF_ERR_ARGUMENT;
   const uint32_t blockouts = NEGF_OUT_GTRANS | NEGF_OUT_GR_LC | NEGF_OUT_GRD | NEGF_OUT_GRL | NEGF_OUT_GRU |
                              NEGF_OUT_GR_LEFT | NEGF_LESSER;
   if ((p->flags & blockouts) && !p->out) return NEGF_ERR_ARGUMENT;

@@ -33,19 +33,6 @@ class DeviceBlocks:
         return [int(h.shape[-1]) for h in self.hd]
 
 
-def _flat(t, dev):
-    return t.to(device=dev, dtype=C128).reshape(-1)
-
-
-def _all_zero(ts, dev):
-    """Which of the tensors are identically zero (one host sync for all)."""
-    if not ts:
-        return []
-    m = torch.stack([t.to(dev).abs().amax() if t.numel() else torch.zeros((), dtype=torch.float64, device=dev)
-                     for t in ts])
-    return (m == 0).tolist()
-
-
 class Geometry:
     """Packed H/S arena + block table for a list of devices (energy independent).
 
@@ -58,21 +45,17 @@ class Geometry:
         dev = torch.device(device)
         self.device = dev
         self.devices = devices
-        pieces, blocks, devs = [], [], []
+        blocks, devs, copies = [], [], []
+        offdiag = []  # (block index, field, arena offset, numel) of H/S coupling blocks
         cursor = 0
 
         def put(t):
             nonlocal cursor
             off = cursor
-            f = _flat(t, dev)
-            pieces.append(f)
-            cursor += f.numel()
+            copies.append((off, t))
+            cursor += t.numel()
             return off
 
-        zero_flags = None
-        if detect_zero_offdiag:
-            offd = [t for d in devices for t in list(d.su) + list(d.sl) + list(d.hu) + list(d.hl)]
-            zero_flags = iter(_all_zero(offd, dev))
         self.max_n = 0
         self.max_g_slab = 0
         for d in devices:
@@ -80,13 +63,6 @@ class Geometry:
             if not (len(d.sd) == K and len(d.hu) == len(d.hl) == len(d.su) == len(d.sl) == K - 1):
                 raise ValueError("inconsistent block lists")
             dims = d.dims
-            if zero_flags is not None:
-                zsu = [next(zero_flags) for _ in d.su]
-                zsl = [next(zero_flags) for _ in d.sl]
-                zhu = [next(zero_flags) for _ in d.hu]
-                zhl = [next(zero_flags) for _ in d.hl]
-            else:
-                zsu = zsl = zhu = zhl = [False] * (K - 1)
             blk0 = len(blocks)
             g = 0
             orb = 0
@@ -103,12 +79,13 @@ class Geometry:
                     b[name] = -1
                 if q + 1 < K:
                     nn = dims[q + 1]
-                    for name, lst, zl, shape in (("hu", d.hu, zhu, (n, nn)), ("su", d.su, zsu, (n, nn)),
-                                                 ("hl", d.hl, zhl, (nn, n)), ("sl", d.sl, zsl, (nn, n))):
+                    for name, lst, shape in (("hu", d.hu, (n, nn)), ("su", d.su, (n, nn)),
+                                             ("hl", d.hl, (nn, n)), ("sl", d.sl, (nn, n))):
                         t = lst[q]
                         if tuple(t.shape[-2:]) != shape:
                             raise ValueError(f"{name}[{q}] has shape {tuple(t.shape)}, expected {shape}")
-                        b[name] = -1 if zl[q] else put(t)
+                        b[name] = put(t)
+                        offdiag.append((len(blocks), name, int(b[name]), t.numel()))
                 b["orb0"] = orb
                 b["g"] = g
                 for f in ("o_grd", "o_grl", "o_gru", "o_grlc", "o_grleft", "o_gnd", "o_gnl", "o_gnu",
@@ -128,9 +105,21 @@ class Geometry:
             self.max_g_slab = max(self.max_g_slab, g)
         if self.max_n > _lib.NEGF_MAX_BLOCK:
             raise ValueError(f"block size {self.max_n} exceeds the supported maximum {_lib.NEGF_MAX_BLOCK}")
-        self.hs = torch.cat(pieces) if pieces else torch.zeros(1, dtype=C128, device=dev)
+        # one host->device copy per block straight into the arena
+        self.hs = torch.empty(max(cursor, 1), dtype=C128, device=dev)
+        for off, t in copies:
+            src = t.detach()
+            if src.dtype != C128:
+                src = src.to(C128)
+            self.hs[off:off + src.numel()].view(src.shape).copy_(src, non_blocking=True)
         self.blocks = np.array(blocks, dtype=_lib.BLOCK_DTYPE)
         self.devs = np.array(devs, dtype=_lib.DEVICE_DTYPE)
+        if detect_zero_offdiag and offdiag:
+            # zero coupling blocks (orthogonal basis: su = sl = 0) are skipped by the kernel
+            amax = torch.stack([self.hs[o:o + n].abs().amax() for _, _, o, n in offdiag])
+            for (bi, name, _, _), z in zip(offdiag, (amax == 0).tolist()):
+                if z:
+                    self.blocks[bi][name] = -1
 
     @property
     def n_orb(self):
@@ -139,10 +128,12 @@ class Geometry:
 
 @dataclass
 class RgfResult:
-    trans: Optional[torch.Tensor]
-    orb_dos: Optional[torch.Tensor]
+    trans: Optional[torch.Tensor]    # [n_items] T(E), item order = device-major, energy-minor
+    orb_dos: Optional[torch.Tensor]  # concatenated per-item [n_orb] -Im diag(GS)/pi
+    dos: Optional[torch.Tensor]      # [n_items] DOS with spin factor 2
     status: torch.Tensor
-    blocks: dict  # per device: tag -> list of [B, ...] tensors (or tensor for g_trans)
+    blocks: list                     # per device: tag -> list of [B, ...] tensors (tensor for g_trans)
+    phase_cycles: Optional[torch.Tensor] = None  # [n_slots, 8] SM cycles per phase
 
 
 _FAMILY = {  # output tag -> (flag, block field, shape fn (n_q, n_next, n_last))
@@ -160,8 +151,8 @@ _FAMILY = {  # output tag -> (flag, block field, shape fn (n_q, n_next, n_last))
 
 def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.Tensor]],
         se_r: List[Optional[torch.Tensor]], eta=0.0, E_ref=0.0, outputs=("g_trans", "grd", "grl", "gru"),
-        trans=False, orb_dos=False, s_in: Optional[List[List[Optional[torch.Tensor]]]] = None,
-        n_slots=None, check=True, stream=None):
+        trans=False, orb_dos=False, dos=False, s_in: Optional[List[List[Optional[torch.Tensor]]]] = None,
+        n_slots=None, check=True, stream=None, phase=False, events=None):
     """Run the batched sweep.
 
     ``energies[d]`` is a 1-D tensor of B_d energies for device d; ``se_l[d]``
@@ -169,6 +160,8 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     names the block tensors to materialise (tags of recursive_gf's tuple);
     ``s_in[d]`` is the per-block list of ``[B_d, n_q, n_q]`` lesser inputs
     (None entries are zero blocks) and switches the lesser sweep on.
+    ``events=(start, end)`` are CUDA events recorded on the launch stream
+    immediately around the kernel (device time of the sweep alone).
     """
     _lib.require_cuda()
     lib = _lib.load()
@@ -190,6 +183,8 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
         flags |= _lib.TRANS
     if orb_dos:
         flags |= _lib.ORB_DOS
+    if dos:
+        flags |= _lib.DOS
     if lesser:
         flags |= _lib.LESSER
 
@@ -197,10 +192,10 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     devs = geom.devs.copy()
     out_cursor = 0
     layout = []  # per device: tag -> list of (offset, shape, B)
-    se_pieces, sin_pieces = [], []
-    se_cursor = 0
+    sin_pieces = []
     sin_cursor = 0
-    items = []
+    item_parts, cost_parts = [], []
+    keep_alive = []
     orb_cursor = 0
     item_cursor = 0
     for d in range(nd):
@@ -228,25 +223,27 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
             lay["g_trans"] = (out_cursor, (dims[0], nl), B)
             out_cursor += B * dims[0] * nl
         layout.append(lay)
-        # self-energies
-        sl_off = sr_off = -1
+        # self-energies are read in place: one device pointer per item
+        ptr_l = ptr_r = 0
         nsl = nsr = 0
-        if se_l[d] is not None:
-            t = se_l[d].to(device=dev, dtype=C128).contiguous()
+        stride_l = stride_r = 0
+        for side in (0, 1):
+            t = (se_l if side == 0 else se_r)[d]
+            if t is None:
+                continue
+            t = t.to(device=dev, dtype=C128)
             if t.ndim == 2:
                 t = t.unsqueeze(0).expand(B, -1, -1)
-            nsl = int(t.shape[-1])
-            sl_off = se_cursor
-            se_pieces.append(t.reshape(-1))
-            se_cursor += B * nsl * nsl
-        if se_r[d] is not None:
-            t = se_r[d].to(device=dev, dtype=C128).contiguous()
-            if t.ndim == 2:
-                t = t.unsqueeze(0).expand(B, -1, -1)
-            nsr = int(t.shape[-1])
-            sr_off = se_cursor
-            se_pieces.append(t.reshape(-1))
-            se_cursor += B * nsr * nsr
+            if t.shape[0] != B or t.shape[-1] != t.shape[-2]:
+                raise ValueError(f"self-energy of shape {tuple(t.shape)} does not match {B} energies")
+            t = t.contiguous() if t.stride(0) != 0 else t[:1].contiguous()
+            keep_alive.append(t)
+            ns = int(t.shape[-1])
+            stride = ns * ns * 16 if t.shape[0] == B and t.stride(0) != 0 else 0
+            if side == 0:
+                ptr_l, nsl, stride_l = t.data_ptr(), ns, stride
+            else:
+                ptr_r, nsr, stride_r = t.data_ptr(), ns, stride
         if lesser:
             for q in range(K):
                 t = s_in[d][q]
@@ -258,37 +255,41 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
                 blocks[b0 + q]["s_in"] = sin_cursor
                 sin_pieces.append(t.reshape(-1))
                 sin_cursor += B * dims[q] * dims[q]
-        z = (E.to(torch.complex128).cpu().numpy() + complex(E_ref)) + 1j * float(eta)
+        z = (E.to(torch.complex128).cpu().numpy().reshape(-1) + complex(E_ref)) + 1j * float(eta)
         n_orb = int(devs[d]["n_orb"])
-        for b in range(B):
-            it = np.zeros((), dtype=_lib.ITEM_DTYPE)
-            it["dev"] = d
-            it["row"] = b
-            it["z_re"] = z[b].real
-            it["z_im"] = z[b].imag
-            it["se_l"] = -1 if sl_off < 0 else sl_off + b * nsl * nsl
-            it["se_r"] = -1 if sr_off < 0 else sr_off + b * nsr * nsr
-            it["nse_l"] = nsl
-            it["nse_r"] = nsr
-            it["out"] = item_cursor
-            it["orb"] = orb_cursor
-            items.append((sum(n ** 3 for n in dims), it))
-            item_cursor += 1
-            orb_cursor += n_orb
-    n_items = len(items)
-    # largest work first (stable: equal costs keep energy order)
-    order = sorted(range(n_items), key=lambda i: -items[i][0])
-    item_arr = np.array([items[i][1] for i in order], dtype=_lib.ITEM_DTYPE)
+        rows = np.arange(B, dtype=np.int64)
+        it = np.zeros(B, dtype=_lib.ITEM_DTYPE)
+        it["dev"] = d
+        it["row"] = rows
+        it["z_re"] = z.real
+        it["z_im"] = z.imag
+        it["se_l"] = (ptr_l + rows * stride_l) if ptr_l else 0
+        it["se_r"] = (ptr_r + rows * stride_r) if ptr_r else 0
+        it["nse_l"] = nsl
+        it["nse_r"] = nsr
+        it["out"] = item_cursor + rows
+        it["orb"] = orb_cursor + rows * n_orb
+        item_parts.append(it)
+        cost_parts.append(np.full(B, sum(n ** 3 for n in dims), dtype=np.int64))
+        item_cursor += B
+        orb_cursor += B * n_orb
+    n_items = item_cursor
+    if n_items:
+        all_items = np.concatenate(item_parts)
+        # largest work first; stable, so equal costs keep energy order
+        item_arr = all_items[np.argsort(-np.concatenate(cost_parts), kind="stable")]
+    else:
+        item_arr = np.zeros(0, dtype=_lib.ITEM_DTYPE)
 
     u8 = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
     blocks_t = u8(blocks)
     devs_t = u8(devs)
     items_t = u8(item_arr) if n_items else torch.zeros(1, dtype=torch.uint8, device=dev)
-    se_t = torch.cat(se_pieces) if se_pieces else torch.zeros(1, dtype=C128, device=dev)
     sin_t = torch.cat(sin_pieces) if sin_pieces else torch.zeros(1, dtype=C128, device=dev)
     out_t = torch.empty(max(out_cursor, 1), dtype=C128, device=dev)
     trans_t = torch.empty(max(item_cursor, 1), dtype=torch.float64, device=dev) if trans else None
     orb_t = torch.empty(max(orb_cursor, 1), dtype=torch.float64, device=dev) if orb_dos else None
+    dos_t = torch.empty(max(item_cursor, 1), dtype=torch.float64, device=dev) if dos else None
     status_t = torch.empty(max(item_cursor, 1), dtype=torch.int32, device=dev)
     if n_slots is None:
         n_slots = max(1, min(n_items, lib.negf_sm_count()))
@@ -300,11 +301,11 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     prob.max_n = geom.max_n
     prob.max_g_slab = geom.max_g_slab
     prob.hs = geom.hs.data_ptr()
-    prob.se = se_t.data_ptr()
     prob.s_in = sin_t.data_ptr()
     prob.out = out_t.data_ptr()
     prob.trans = trans_t.data_ptr() if trans else None
     prob.orb_dos = orb_t.data_ptr() if orb_dos else None
+    prob.dos = dos_t.data_ptr() if dos else None
     prob.status = status_t.data_ptr()
     prob.flags = flags
     prob.n_slots = n_slots
@@ -312,9 +313,17 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     scratch = torch.empty(max(need, 256), dtype=torch.uint8, device=dev)
     prob.scratch = scratch.data_ptr()
     prob.scratch_bytes = scratch.numel()
+    phase_t = None
+    if phase:
+        phase_t = torch.zeros((n_slots, len(_lib.PHASES)), dtype=torch.int64, device=dev)
+        prob.phase_cycles = phase_t.data_ptr()
     # the staging tensors may be released on return: the caching allocator
     # only hands their memory to work ordered after this launch on the stream
+    if events is not None:
+        events[0].record(stream)
     _lib.check(lib.negf_rgf_run(ctypes.byref(prob), _lib.stream_handle(stream)), "negf_rgf_run")
+    if events is not None:
+        events[1].record(stream)
 
     res_blocks = []
     for d in range(nd):
@@ -338,4 +347,5 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
             raise _lib.NegfError(f"RGF failed for item {bad} with status {code}")
     return RgfResult(trans=trans_t[:item_cursor] if trans else None,
                      orb_dos=orb_t[:orb_cursor] if orb_dos else None,
-                     status=status_t[:item_cursor], blocks=res_blocks)
+                     dos=dos_t[:item_cursor] if dos else None,
+                     status=status_t[:item_cursor], blocks=res_blocks, phase_cycles=phase_t)

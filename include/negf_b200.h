@@ -52,6 +52,10 @@ extern "C" {
 #define NEGF_TRANS (1u << 6)       /* T(E) = Re Tr[G_L G_1N G_R G_1N^H] -> trans[]  */
 #define NEGF_ORB_DOS (1u << 7)     /* -Im diag(G S)_i / pi per orbital -> orb_dos[] */
 #define NEGF_LESSER (1u << 8)      /* lesser sweep: gin_left, gnd, gnl, gnu          */
+#define NEGF_DOS (1u << 9)         /* DOS = 2 sum_i (-Im diag(G S)_i / pi) -> dos[]  */
+
+/* Phase indices of NegfRgfProblem.phase_cycles (clock64 cycles per slot). */
+#define NEGF_PHASES 8 /* form, gemm_fwd, inverse, gemm_bwd, lesser, dos, trans, other */
 
 /* One diagonal block q of a block-tridiagonal device. */
 typedef struct NegfBlock {
@@ -85,8 +89,8 @@ typedef struct NegfItem {
   int32_t row;     /* batch row of this energy within the device's outputs */
   double z_re;     /* z = E + E_ref + i*eta (recursive_green_cal.py:75,:378) */
   double z_im;
-  int64_t se_l;    /* offset of Sigma_L [nse_l x nse_l] in se; -1 = none */
-  int64_t se_r;    /* offset of Sigma_R [nse_r x nse_r] in se; -1 = none */
+  const double* se_l; /* Sigma_L [nse_l x nse_l] complex128 (device memory); NULL = none */
+  const double* se_r; /* Sigma_R [nse_r x nse_r] complex128 (device memory); NULL = none */
   int32_t nse_l, nse_r;
   int64_t out;     /* index into trans[] and status[] */
   int64_t orb;     /* offset (doubles) of this item's n_orb entries in orb_dos[] */
@@ -100,16 +104,17 @@ typedef struct NegfRgfProblem {
   int32_t max_n;            /* largest n_q over all devices (<= NEGF_MAX_BLOCK) */
   int64_t max_g_slab;       /* largest g slab over all devices */
   const double* hs;         /* complex128 arena of H/S blocks */
-  const double* se;         /* complex128 arena of self-energies */
   const double* s_in;       /* complex128 arena of Sigma^in blocks (NEGF_LESSER) */
   double* out;              /* complex128 arena of block outputs */
   double* trans;            /* [n_items] T(E) (NEGF_TRANS) */
   double* orb_dos;          /* per-orbital -Im diag(GS)/pi (NEGF_ORB_DOS) */
+  double* dos;              /* [n_items] DOS with spin factor 2 (NEGF_DOS) */
   int32_t* status;          /* [n_items] per-item status (always written) */
   uint32_t flags;
   int32_t n_slots;          /* concurrent work slots = CTAs launched */
   void* scratch;            /* >= negf_rgf_scratch_bytes(problem) bytes, 256-aligned */
   size_t scratch_bytes;
+  unsigned long long* phase_cycles; /* optional [n_slots x NEGF_PHASES] SM-cycle counters; NULL = off */
 } NegfRgfProblem;
 
 /* Bytes of scratch negf_rgf_run needs for p->n_slots, p->max_n, p->max_g_slab, p->flags. */

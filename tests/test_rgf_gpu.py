@@ -113,7 +113,7 @@ def test_fused_transmission_and_dos(dims):
     dev, seL, seR, E, _ = _oracle_case(dims, B, seed=5)
     geom = rgf_plan.Geometry([rgf_plan.DeviceBlocks(dev.hd, dev.hu, dev.hl, dev.sd, dev.su, dev.sl)])
     res = rgf_plan.run(geom, [E.cuda()], [seL.cuda()], [seR.cuda()], eta=1e-5, outputs=(),
-                       trans=True, orb_dos=True)
+                       trans=True, orb_dos=True, dos=True)
     ref = rgf_oracle.rgf(E.numpy(), [x.numpy() for x in dev.hl], [x.numpy() for x in dev.hd],
                          [x.numpy() for x in dev.hu], [x.numpy() for x in dev.sd],
                          [x.numpy() for x in dev.su], [x.numpy() for x in dev.sl],
@@ -126,6 +126,29 @@ def test_fused_transmission_and_dos(dims):
     got_dos = 2.0 * res.orb_dos.cpu().numpy().reshape(B, -1).sum(-1)
     np.testing.assert_allclose(got_T, T, rtol=1e-10, atol=1e-12)
     np.testing.assert_allclose(got_dos, dos, rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(res.dos.cpu().numpy(), dos, rtol=1e-10, atol=1e-12)
+
+
+def test_transport_api_host_tensors():
+    """Public fused API with host inputs returns host T/DOS equal to the oracle."""
+    from dpnegf_b200 import transport
+    dims = [48, 48, 48]
+    B = 5
+    dev, seL, seR, E, _ = _oracle_case(dims, B, seed=21)
+    T, D, orb = transport.transmission_dos(dev.hd, dev.hu, dev.hl, dev.sd, dev.su, dev.sl, E, seL, seR,
+                                           eta=1e-5, E_ref=0.02, orbital_dos=True)
+    assert T.device.type == "cpu" and D.device.type == "cpu" and orb.shape == (B, sum(dims))
+    ref = rgf_oracle.rgf(E.numpy(), [x.numpy() for x in dev.hl], [x.numpy() for x in dev.hd],
+                         [x.numpy() for x in dev.hu], [x.numpy() for x in dev.sd],
+                         [x.numpy() for x in dev.su], [x.numpy() for x in dev.sl],
+                         seL.numpy(), seR.numpy(), eta=1e-5, E_ref=0.02)
+    Tr = rgf_oracle.transmission(ref["g_trans"], rgf_oracle.gamma_from_se(seL.numpy()),
+                                 rgf_oracle.gamma_from_se(seR.numpy()))
+    Dr = rgf_oracle.dos(ref["grd"], ref["grl"], ref["gru"], [x.numpy() for x in dev.sd],
+                        [x.numpy() for x in dev.su], [x.numpy() for x in dev.sl])
+    np.testing.assert_allclose(T.numpy(), Tr, rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(D.numpy(), Dr, rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(2 * orb.numpy().sum(-1), Dr, rtol=1e-10, atol=1e-12)
 
 
 def test_chain_transmission_is_one_in_band():

@@ -1,0 +1,72 @@
+"""Fused T(E)/DOS sweep through ``negf_rgf_run_static`` (include/negf_b200.h).
+
+For callers that cannot allocate device memory while the sweep runs (a host
+transport code that owns the GPU through its own pool, or a plugin that only
+receives input and output buffers): the library takes its scratch from a fixed
+64 MiB array per GPU instead of a caller buffer.  The descriptor tables and
+the output tensors are still the caller's; this helper builds them with torch
+before the call, the C entry point itself allocates nothing.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from .rgf_plan import Geometry
+
+NEGF_ERR_SCRATCH_LIMIT = -4
+
+
+def _bind(lib):
+    lib.negf_rgf_run_static.restype = ctypes.c_int
+    lib.negf_rgf_run_static.argtypes = [ctypes.POINTER(_lib.NegfRgfProblem), ctypes.c_void_p]
+    lib.negf_rgf_static_scratch_bytes.restype = ctypes.c_size_t
+    lib.negf_rgf_static_scratch_bytes.argtypes = []
+    return lib
+
+
+def static_scratch_bytes():
+    return int(_bind(_lib.load()).negf_rgf_static_scratch_bytes())
+
+
+def transmission_dos_static(geom: Geometry, energy: torch.Tensor, left_se: torch.Tensor,
+                            right_se: torch.Tensor, eta=0.0, E_ref=0.0, n_slots=None, stream=None):
+    """T(E) and DOS of the single device in ``geom`` at ``energy`` ([B]); returns (T, DOS, status, code).
+
+    ``code`` is the call-level status of negf_rgf_run_static (0 on success).
+    """
+    _lib.require_cuda()
+    lib = _bind(_lib.load())
+    if len(geom.devs) != 1:
+        raise ValueError("one device per call")
+    dev = geom.device
+    B = int(energy.shape[0])
+    seL = left_se.to(device=dev, dtype=torch.complex128).contiguous()
+    seR = right_se.to(device=dev, dtype=torch.complex128).contiguous()
+    z = energy.to(torch.complex128).cpu().numpy().reshape(-1) + complex(E_ref) + 1j * float(eta)
+    rows = np.arange(B, dtype=np.int64)
+    items = np.zeros(B, dtype=_lib.ITEM_DTYPE)
+    items["row"] = rows
+    items["z_re"], items["z_im"] = z.real, z.imag
+    nsl, nsr = int(seL.shape[-1]), int(seR.shape[-1])
+    items["se_l"] = seL.data_ptr() + rows * nsl * nsl * 16
+    items["se_r"] = seR.data_ptr() + rows * nsr * nsr * 16
+    items["nse_l"], items["nse_r"] = nsl, nsr
+    items["out"] = rows
+    u8 = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
+    blocks_t, devs_t, items_t = u8(geom.blocks), u8(geom.devs), u8(items)
+    T = torch.empty(B, dtype=torch.float64, device=dev)
+    D = torch.empty(B, dtype=torch.float64, device=dev)
+    status = torch.empty(B, dtype=torch.int32, device=dev)
+    p = _lib.NegfRgfProblem()
+    p.blocks, p.devices, p.items = blocks_t.data_ptr(), devs_t.data_ptr(), items_t.data_ptr()
+    p.n_items, p.max_n, p.max_g_slab = B, geom.max_n, geom.max_g_slab
+    p.hs = geom.hs.data_ptr()
+    p.trans, p.dos, p.status = T.data_ptr(), D.data_ptr(), status.data_ptr()
+    p.flags = _lib.TRANS | _lib.DOS
+    p.n_slots = n_slots or max(1, min(B, lib.negf_sm_count()))
+    code = lib.negf_rgf_run_static(ctypes.byref(p), _lib.stream_handle(stream))
+    torch.cuda.current_stream(dev).synchronize()
+    del blocks_t, devs_t, items_t
+    return T, D, status, code

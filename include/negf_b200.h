@@ -39,6 +39,7 @@ extern "C" {
 #define NEGF_ERR_ARGUMENT -1        /* malformed descriptor (call-level) */
 #define NEGF_ERR_UNSUPPORTED -2     /* block size above the compiled maximum (call-level) */
 #define NEGF_ERR_CUDA -3            /* CUDA launch / attribute error (call-level) */
+#define NEGF_ERR_SCRATCH_LIMIT -4   /* negf_rgf_run_static: one work slot needs more than the static array */
 
 #define NEGF_MAX_BLOCK 512 /* largest diagonal block the kernels accept */
 
@@ -128,6 +129,24 @@ size_t negf_rgf_scratch_bytes(const NegfRgfProblem* p);
  * diagonal (:408-470) are reduced inside the sweep.  Returns a call-level
  * status; per-item status in p->status. */
 int negf_rgf_run(const NegfRgfProblem* p, void* cuda_stream);
+
+/* negf_rgf_run for callers that cannot allocate device memory (no counterpart
+ * in the reference, which allocates through torch on every call).  A host code
+ * that embeds the sweep in its own solver loop often owns the GPU through its
+ * own memory pool or receives only input/output buffers, and cudaMalloc would
+ * synchronise the device or fail there.  This entry point takes its scratch
+ * from a 64 MiB array inside the library (one per GPU, kept until exit)
+ * instead of p->scratch / p->scratch_bytes, which are ignored, and allocates
+ * nothing.  Inputs and outputs are still the caller's.  The slot count is
+ * lowered to what fits; a problem whose single slot does not fit returns
+ * NEGF_ERR_SCRATCH_LIMIT.  All calls on a GPU share the array (the work-queue
+ * counter is cleared on entry; overlapping calls on the GPU race), and the
+ * first call on a device resolves the array's address, so make it before any
+ * stream capture. */
+int negf_rgf_run_static(const NegfRgfProblem* p, void* cuda_stream);
+
+/* Size in bytes of the static scratch array used by negf_rgf_run_static. */
+size_t negf_rgf_static_scratch_bytes(void);
 
 /* Number of SMs of the current CUDA device (grid sizing helper). */
 int negf_sm_count(void);

@@ -35,10 +35,11 @@ TRANS = 1 << 6
 ORB_DOS = 1 << 7
 LESSER = 1 << 8
 DOS = 1 << 9
-PHASES = ("form", "gemm_fwd", "inverse", "gemm_bwd", "lesser", "dos", "trans", "other")
+PHASES = ("form", "gemm_fwd", "inv_stage", "inv_panel", "inv_update", "inv_gather", "gemm_bwd", "lesser",
+          "dos", "trans", "other")
 
 # numpy mirrors of the descriptor structs (packed exactly like the C structs)
-BLOCK_FIELDS = ["hd", "sd", "hu", "su", "hl", "sl", "orb0", "g", "o_grd", "o_grl", "o_gru", "o_grlc",
+BLOCK_FIELDS = ["hd", "sd", "hu", "su", "hl", "sl", "sdT", "suT", "slT", "orb0", "g", "o_grd", "o_grl", "o_gru", "o_grlc",
                 "o_grleft", "o_gnd", "o_gnl", "o_gnu", "o_ginleft", "s_in"]
 BLOCK_DTYPE = np.dtype([("n", "<i4"), ("n_next", "<i4")] + [(f, "<i8") for f in BLOCK_FIELDS])
 DEVICE_DTYPE = np.dtype([("n_blocks", "<i4"), ("blk0", "<i4"), ("n_orb", "<i4"), ("pad", "<i4"),

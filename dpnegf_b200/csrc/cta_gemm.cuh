@@ -19,7 +19,8 @@ constexpr int GT_M = 64, GT_N = 64, GT_K = 16;
 constexpr int PITCH_MK = GT_K + 4;  // [64 rows][16 k] tiles (pitch = 4 mod 8)
 constexpr int PITCH_KN = GT_N + 2;  // [16 k][64 cols] tiles (pitch = 2 mod 8)
 constexpr int GT_TILE = (GT_M * PITCH_MK > GT_K * PITCH_KN) ? GT_M * PITCH_MK : GT_K * PITCH_KN;
-constexpr int GEMM_SMEM_BYTES = 4 * GT_TILE * (int)sizeof(cplx);  // 2 stages x (A,B)
+constexpr int GT_STAGES = 3;
+constexpr int GEMM_SMEM_BYTES = 2 * GT_STAGES * GT_TILE * (int)sizeof(cplx);  // stages x (A,B)
 constexpr int CTA_THREADS = 256;
 
 struct GemmArgs {
@@ -164,52 +165,70 @@ struct AIdxOpC { NEGF_DEV int operator()(int m, int k) const { return a_idx<OP_C
 struct BIdxOp0 { NEGF_DEV int operator()(int k, int n) const { return b_idx<OP_N>(k, n); } };
 struct BIdxOpC { NEGF_DEV int operator()(int k, int n) const { return b_idx<OP_C>(k, n); } };
 
-// C = alpha op(A) op(B) + beta D over the whole matrix, by the whole CTA.
-// C must not alias A or B.  Ends with __syncthreads(), so C is visible to
-// every thread of the CTA on return.
-template <int OPA, int OPB>
-NEGF_DEV void cta_gemm(const GemmArgs& g, cplx* smem) {
+// Default epilogue: C = alpha * acc + beta * D.
+struct EpiStore {
+  GemmArgs g;
+  NEGF_DEV void operator()(int m, int n, cplx v) const {
+    cplx o = cmul(g.alpha, v);
+    if (g.use_d) o = cfma(g.beta, g.D[(int64_t)m * g.ldd + n], o);
+    g.C[(int64_t)m * g.ldc + n] = o;
+  }
+};
+
+// acc = op(A) op(B) over the whole M x N output by the whole CTA; epi(m, n, acc)
+// is called once for every in-range element.  The output must not alias A or
+// B.  Ends with __syncthreads(), so whatever epi wrote to global memory is
+// visible to every thread of the CTA on return.  k-slabs flow through a
+// GT_STAGES-deep cp.async ring (one barrier per slab).
+template <int OPA, int OPB, class Epi>
+__device__ __noinline__ void cta_gemm_epi(const GemmArgs g, cplx* smem, const Epi epi) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = (warp >> 2) * 32, wn = (warp & 3) * 16;
-  cplx* sA[2] = {smem, smem + GT_TILE};
-  cplx* sB[2] = {smem + 2 * GT_TILE, smem + 3 * GT_TILE};
   const int nk = (g.K + GT_K - 1) / GT_K;
   typedef typename std::conditional<OPA == OP_C, AIdxOpC, AIdxOp0>::type AI;
   typedef typename std::conditional<OPB == OP_C, BIdxOpC, BIdxOp0>::type BI;
   constexpr bool CA = (OPA != OP_N), CB = (OPB != OP_N);
+  auto sA = [&](int s) { return smem + (2 * s) * GT_TILE; };
+  auto sB = [&](int s) { return smem + (2 * s + 1) * GT_TILE; };
 
   for (int m0 = 0; m0 < g.M; m0 += GT_M) {
     for (int n0 = 0; n0 < g.N; n0 += GT_N) {
-      Acc3M acc;
-      acc.zero();
-      if (nk > 0) {
-        load_a_tile<OPA>(sA[0], g, m0, 0, tid);
-        load_b_tile<OPB>(sB[0], g, 0, n0, tid);
-      }
-      cp_async_commit();
-      for (int kt = 0; kt < nk; ++kt) {
-        if (kt + 1 < nk) {
-          load_a_tile<OPA>(sA[(kt + 1) & 1], g, m0, (kt + 1) * GT_K, tid);
-          load_b_tile<OPB>(sB[(kt + 1) & 1], g, (kt + 1) * GT_K, n0, tid);
+      __syncthreads();  // the previous tile's last slab is no longer being read
+#pragma unroll
+      for (int s = 0; s < GT_STAGES - 1; ++s) {
+        if (s < nk) {
+          load_a_tile<OPA>(sA(s), g, m0, s * GT_K, tid);
+          load_b_tile<OPB>(sB(s), g, s * GT_K, n0, tid);
         }
         cp_async_commit();
-        cp_async_wait<1>();
+      }
+      Acc3M acc;
+      acc.zero();
+      for (int kt = 0; kt < nk; ++kt) {
+        cp_async_wait<GT_STAGES - 2>();
         __syncthreads();
-        warp_mma_3m<CA, CB>(acc, sA[kt & 1], sB[kt & 1], GT_K / 4, wm, wn, lane, AI(), BI());
-        __syncthreads();
+        const int nx = kt + GT_STAGES - 1;
+        if (nx < nk) {
+          load_a_tile<OPA>(sA(nx % GT_STAGES), g, m0, nx * GT_K, tid);
+          load_b_tile<OPB>(sB(nx % GT_STAGES), g, nx * GT_K, n0, tid);
+        }
+        cp_async_commit();
+        warp_mma_3m<CA, CB>(acc, sA(kt % GT_STAGES), sB(kt % GT_STAGES), GT_K / 4, wm, wn, lane, AI(), BI());
       }
       acc_foreach(acc, wm, wn, lane, [&](int r, int c, cplx v) {
         int m = m0 + r, n = n0 + c;
-        if (m < g.M && n < g.N) {
-          cplx o = cmul(g.alpha, v);
-          if (g.use_d) o = cfma(g.beta, g.D[(int64_t)m * g.ldd + n], o);
-          g.C[(int64_t)m * g.ldc + n] = o;
-        }
+        if (m < g.M && n < g.N) epi(m, n, v);
       });
     }
   }
   cp_async_wait<0>();
   __syncthreads();
+}
+
+// C = alpha op(A) op(B) + beta D (D may alias C; C must not alias A or B).
+template <int OPA, int OPB>
+NEGF_DEV void cta_gemm(const GemmArgs& g, cplx* smem) {
+  cta_gemm_epi<OPA, OPB>(g, smem, EpiStore{g});
 }
 
 }  // namespace negf

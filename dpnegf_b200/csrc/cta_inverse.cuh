@@ -1,5 +1,5 @@
-// CTA-wide complex128 matrix inverse: blocked Gauss-Jordan with partial
-// pivoting, rank-NB updates on FP64 tensor cores.
+// CTA-wide complex128 matrix inverse: two-level blocked Gauss-Jordan with
+// partial pivoting on FP64 tensor cores.
 //
 // The matrix W (n x n, row stride ldw) is a work buffer in global memory and
 // is destroyed; the inverse is written to G.  Pivoting is implicit: rows never
@@ -9,37 +9,51 @@
 // in place: column c of W holds column p(c) of T.  Since row i of A^-1 is row
 // p(i) of T, the inverse is recovered by the gather
 //     G[i][j] = W[p(i)][p^-1(j)],
-// fused into the final store.  Each panel of NB columns is factorised in
-// shared memory (one warp row-group per row, one lane per column, warp-level
-// argmax for the pivot) and then applied to every other column as
-//     W[:, c] <- P * W[pivots, c] + (W[:, c] with the pivot rows zeroed),
-// a GEMM with k = NB whose A operand (the factorised panel P) already sits in
-// shared memory.  Work: n^3 complex multiply-adds, as for an explicit inverse
+// fused into the final store.
+//
+// Blocking.  Columns are taken in outer blocks of OB = 128 (the whole matrix
+// when n <= 128).  Inside a block, panels of NB columns are factorised in
+// shared memory and applied to the block's other columns only (rank-NB
+// updates, k = NB).  The finished block transform is then applied to every
+// column outside the block with one GEMM of depth k = OB at full tile-GEMM
+// efficiency:
+//     W[:, c] <- W[:, block] * W[block pivots, c] + (W[:, c] with the block's pivot rows zeroed),
+// reading the block's pivot rows from a snapshot (they are overwritten by the
+// same update).  Work: n^3 complex multiply-adds, as for an explicit inverse
 // by LU.
+//
+// Panel factorisation in registers: every thread holds whole panel rows
+// (row tid + 256 r, NB complex entries), so a column step is one broadcast of
+// the scaled pivot row through shared memory and register-only updates; the
+// pivot search for the next column uses the entries each thread just
+// produced.  Two barriers per column.
 #pragma once
 #include "cta_gemm.cuh"
 
 namespace negf {
 
+constexpr int INV_OB = 128;  // outer block (columns) of the two-level Gauss-Jordan
+
 template <int NB>
 struct InvLayout {
   static constexpr int PP = NB + 4;  // panel pitch (= 4 mod 8: conflict-free A fragments)
   static constexpr int RP = GT_N + 2;
-  NEGF_DEV static int rows(int n) { return (n + GT_M - 1) / GT_M * GT_M; }
-  NEGF_DEV static size_t bytes(int n) {
-    size_t b = (size_t)rows(n) * PP * sizeof(cplx) + (size_t)NB * RP * sizeof(cplx);
+  __host__ __device__ static int rows(int n) { return (n + GT_M - 1) / GT_M * GT_M; }
+  __host__ __device__ static size_t bytes(int n) {
+    size_t b = (size_t)rows(n) * PP * sizeof(double2) + 2 * (size_t)NB * RP * sizeof(double2);
+    b += 2 * (size_t)rows(n) * sizeof(double2) + NB * sizeof(double2);  // multiplier columns, spare row
     b += (size_t)(2 * n + 64) * sizeof(int) + 16 * sizeof(double);
     return b;
   }
 };
 
 inline size_t inv_smem_bytes_host(int n) {
-  const int NB = n <= 256 ? 32 : 16;
-  const int rows = (n + GT_M - 1) / GT_M * GT_M;
-  size_t b = (size_t)rows * (NB + 4) * sizeof(double2) + (size_t)NB * (GT_N + 2) * sizeof(double2);
-  b += (size_t)(2 * n + 64) * sizeof(int) + 16 * sizeof(double);
-  return b;
+  size_t a = n <= 256 ? InvLayout<32>::bytes(n) : InvLayout<16>::bytes(n);
+  return a > (size_t)GEMM_SMEM_BYTES ? a : (size_t)GEMM_SMEM_BYTES;  // the outer update runs the tile GEMM
 }
+
+// Complex elements of the pivot-row snapshot the inverse needs (INV_OB x n).
+__host__ __device__ inline size_t inv_snapshot_elems(int n) { return (size_t)INV_OB * n; }
 
 struct PanelIdx {
   int pitch;
@@ -49,146 +63,284 @@ struct RIdx {
   NEGF_DEV int operator()(int k, int n) const { return k * (GT_N + 2) + n; }
 };
 
+// argmax over (value, index) pairs: larger value wins, ties go to the lower index
+NEGF_DEV void argmax_merge(double& v, int& i, double ov, int oi) {
+  if (ov > v || (ov == v && oi < i)) { v = ov; i = oi; }
+}
+NEGF_DEV void warp_argmax(double& v, int& i) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    double ov = __shfl_xor_sync(0xffffffffu, v, off);
+    int oi = __shfl_xor_sync(0xffffffffu, i, off);
+    argmax_merge(v, i, ov, oi);
+  }
+}
+NEGF_DEV double pivot_measure(cplx a) {
+  double v = cabs1(a);
+  return (v == v) ? v : INFINITY;  // NaN pivots are taken (and flagged) first
+}
+
+// Outer-update epilogue: pivot rows of the block take the product, the other
+// rows add it to their current value.
+struct EpiGJ {
+  cplx* W;
+  int64_t ldw;
+  const int* pinv;
+  int c_lo, c_hi, col0;
+  NEGF_DEV void operator()(int m, int n, cplx v) const {
+    cplx* dst = W + (int64_t)m * ldw + col0 + n;
+    const int lc = pinv[m];
+    *dst = (lc >= c_lo && lc < c_hi) ? v : cadd(*dst, v);
+  }
+};
+
 // Returns 0 on success, 1 if a zero or non-finite pivot was met.  Uniform
-// across the CTA; ends with __syncthreads().
-template <int NB>
-NEGF_DEV int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G, int64_t ldg, char* smem_raw) {
+// across the CTA; ends with __syncthreads().  `snap` is global scratch of
+// inv_snapshot_elems(n) complex elements (unused when n <= INV_OB).
+template <int NB, int RT>
+__device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G, int64_t ldg, char* smem_raw,
+                                           PhaseClock* pc, cplx* snap) {
   constexpr int PP = InvLayout<NB>::PP;
   constexpr int RP = InvLayout<NB>::RP;
   constexpr int NWARP = CTA_THREADS / 32;
-  constexpr int ROWS_PER_PASS = CTA_THREADS / NB;  // rows updated concurrently
+  static_assert(NB * RT == 32, "a thread holds RT panel rows of NB complex entries");
+  const int n_pad = InvLayout<NB>::rows(n);
   cplx* P = reinterpret_cast<cplx*>(smem_raw);
-  const int n_pad = InvLayout<NB>::rows(n);  // panel rows padded to the 64-row tiles
-  cplx* R = P + (size_t)n_pad * PP;
-  int* piv = reinterpret_cast<int*>(R + NB * RP);  // logical column -> physical row
-  int* pinv = piv + n;                             // physical row -> logical column (-1: unused)
-  int* red_i = pinv + n;                           // [NWARP]
-  int* s_misc = red_i + NWARP;                     // [0]: pivot row, [1]: singular flag
-  double* red_v = reinterpret_cast<double*>(s_misc + 56);  // [NWARP], 8-byte aligned
+  cplx* Rb[2] = {P + (size_t)n_pad * PP, P + (size_t)n_pad * PP + NB * RP};
+  cplx* qrow = Rb[1] + NB * RP;  // [NB] published pivot row of the current column
+  int* piv = reinterpret_cast<int*>(qrow + 2 * n_pad + NB);  // logical column -> physical row
+  int* pinv = piv + n;                           // physical row -> logical column (-1: unused)
+  int* red_i = pinv + n;                         // [2][NWARP] pivot candidates (double buffered)
+  int* s_misc = red_i + 2 * NWARP;               // [1]: singular flag
+  double* red_v = reinterpret_cast<double*>(s_misc + 48);  // [2][NWARP]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int my_col = tid % NB, my_rg = tid / NB;
+  const int wm = (warp >> 2) * 32, wn = (warp & 3) * 16;
+  const int gr = lane >> 2, gc = lane & 3;
+  // Panel rows owned by this thread: tid + 256 r, r < RT (n <= 256 RT).
+  // Bit r of `used` is set once that row has served as a pivot.
+  unsigned used = 0u;
+  int par = 0;
 
   for (int i = tid; i < n; i += CTA_THREADS) pinv[i] = -1;
   if (tid == 0) s_misc[1] = 0;
   __syncthreads();
 
-  for (int p0 = 0; p0 < n; p0 += NB) {
-    const int w = min(NB, n - p0);
-    // ---- stage the panel W[:, p0:p0+w) (zero padded to NB columns, n_pad rows)
-    for (int e = tid; e < n_pad * NB; e += CTA_THREADS) {
-      int i = e / NB, jj = e % NB;
-      P[i * PP + jj] = (jj < w && i < n) ? W[(int64_t)i * ldw + p0 + jj] : cmk(0.0, 0.0);
-    }
+  // Every thread merges the per-warp candidates (one barrier per pivot) and
+  // marks the winner as used; thread 0 records it for the updates and gather.
+  auto choose_pivot = [&](double v, int i, int c) -> int {
+    warp_argmax(v, i);
+    if (lane == 0) { red_v[par * NWARP + warp] = v; red_i[par * NWARP + warp] = i; }
     __syncthreads();
-
-    // ---- unblocked Gauss-Jordan on the panel
-    for (int jj = 0; jj < w; ++jj) {
-      const int c = p0 + jj;
-      // pivot search over unused rows
-      double best = -1.0;
-      int bidx = n;
-      for (int i = tid; i < n; i += CTA_THREADS) {
-        if (pinv[i] < 0) {
-          double v = cabs1(P[i * PP + jj]);
-          if (!(v == v)) v = INFINITY;  // NaN pivots are taken (and flagged) first
-          if (v > best || (v == best && i < bidx)) { best = v; bidx = i; }
-        }
-      }
+    double bv = red_v[par * NWARP];
+    int bi = red_i[par * NWARP];
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        double ov = __shfl_down_sync(0xffffffffu, best, off);
-        int oi = __shfl_down_sync(0xffffffffu, bidx, off);
-        if (ov > best || (ov == best && oi < bidx)) { best = ov; bidx = oi; }
+    for (int k = 1; k < NWARP; ++k) argmax_merge(bv, bi, red_v[par * NWARP + k], red_i[par * NWARP + k]);
+    par ^= 1;
+    if (tid == 0) {
+      if (!(bv > 0.0) || !isfinite(bv)) s_misc[1] = 1;
+      piv[c] = bi;
+      pinv[bi] = c;
+    }
+    if (bi % CTA_THREADS == tid) used |= 1u << (bi / CTA_THREADS);
+    return bi;
+  };
+
+  const int ob = n <= INV_OB ? n : INV_OB;
+  for (int c_lo = 0; c_lo < n; c_lo += ob) {
+    const int c_hi = min(c_lo + ob, n);
+    for (int p0 = c_lo; p0 < c_hi; p0 += NB) {
+      const int w = min(NB, c_hi - p0);
+      // ---- stage the panel W[:, p0:p0+w) (zero padded to NB columns, n_pad rows)
+      for (int e = tid; e < n_pad * NB; e += CTA_THREADS) {
+        int i = e / NB, jj = e % NB;
+        bool v = (jj < w && i < n);
+        cp_async16(P + i * PP + jj, v ? W + (int64_t)i * ldw + p0 + jj : W, v);
       }
-      if (lane == 0) { red_v[warp] = best; red_i[warp] = bidx; }
+      cp_async_commit();
+      cp_async_wait<0>();
       __syncthreads();
-      if (tid == 0) {
-        double bv = red_v[0];
-        int bi = red_i[0];
-        for (int k = 1; k < NWARP; ++k)
-          if (red_v[k] > bv || (red_v[k] == bv && red_i[k] < bi)) { bv = red_v[k]; bi = red_i[k]; }
-        if (!(bv > 0.0) || !isfinite(bv)) s_misc[1] = 1;
-        piv[c] = bi;
-        pinv[bi] = c;
-        s_misc[0] = bi;
+      // each thread takes its rows (tid + 256 r) of the panel into registers
+      cplx row[RT][NB];
+      cplx mm[RT];  // the rows' entries in the column being eliminated
+      double bv = -1.0;
+      int bi = n;
+#pragma unroll
+      for (int r = 0; r < RT; ++r) {
+        const int i = tid + CTA_THREADS * r;
+#pragma unroll
+        for (int k = 0; k < NB; ++k) row[r][k] = (i < n) ? P[i * PP + k] : cmk(0.0, 0.0);
+        mm[r] = row[r][0];
+        if (i < n && !((used >> r) & 1u)) argmax_merge(bv, bi, pivot_measure(mm[r]), i);
       }
-      __syncthreads();
-      const int p = s_misc[0];
-      const cplx d = crcp(P[p * PP + jj]);
-      const cplx pd = cmul(P[p * PP + my_col], d);  // scaled pivot row, my column
-      __syncthreads();  // pivot row / column jj are rewritten below
-      // warp-uniform trip count: every lane reaches each __syncwarp
-      for (int base = 0; base < n; base += ROWS_PER_PASS) {
-        const int i = base + my_rg;
-        const bool act = i < n;
-        const cplx f = act ? P[i * PP + jj] : cmk(0.0, 0.0);
-        const cplx x = act ? P[i * PP + my_col] : cmk(0.0, 0.0);
-        __syncwarp();
-        if (act && my_col < w) {
-          cplx o;
-          if (i == p) o = (my_col == jj) ? d : pd;
-          else o = (my_col == jj) ? cneg(cmul(f, d)) : csub(x, cmul(f, pd));
-          P[i * PP + my_col] = o;
+      int p = choose_pivot(bv, bi, p0);
+      pc->mark(PH_INV_STAGE);
+
+      // ---- unblocked Gauss-Jordan on the panel, in registers.  Column jj:
+      // the pivot row's owner publishes q_k = P[p][k]/P[p][jj] (q_jj = 1/P[p][jj])
+      // and keeps it as its row; every other row i does
+      //     P[i][k] <- (k == jj ? 0 : P[i][k]) - m_i q_k,   m_i = P[i][jj],
+      // and hands the next column's entry to the pivot search.
+      for (int jj = 0; jj < w; ++jj) {
+#pragma unroll
+        for (int r = 0; r < RT; ++r) {
+          if (tid + CTA_THREADS * r == p) {
+            const cplx d = crcp(mm[r]);
+#pragma unroll
+            for (int k = 0; k < NB; ++k) {
+              const cplx q = (k == jj) ? d : cmul(row[r][k], d);
+              row[r][k] = q;
+              qrow[k] = q;
+            }
+          }
         }
-        __syncwarp();
+        __syncthreads();
+        const int nxt = jj + 1;
+        bv = -1.0;
+        bi = n;
+#pragma unroll
+        for (int r = 0; r < RT; ++r) {
+          const int i = tid + CTA_THREADS * r;
+          cplx mnext = cmk(0.0, 0.0);
+          if (i < n) {
+            if (i != p) {
+              const cplx m = mm[r];
+#pragma unroll
+              for (int k = 0; k < NB; ++k) {
+                const cplx q = qrow[k];
+                const cplx x = (k == jj) ? cmk(0.0, 0.0) : row[r][k];
+                const cplx o = csub(x, cmul(m, q));
+                row[r][k] = o;
+                if (k == nxt) mnext = o;
+              }
+            } else {
+#pragma unroll
+              for (int k = 0; k < NB; ++k)
+                if (k == nxt) mnext = row[r][k];
+            }
+            if (nxt < w && i != p && !((used >> r) & 1u)) argmax_merge(bv, bi, pivot_measure(mnext), i);
+          }
+          mm[r] = mnext;
+        }
+        if (nxt < w) p = choose_pivot(bv, bi, p0 + nxt);
+        else __syncthreads();  // qrow is rewritten by the next panel's first column
+      }
+      // the factorised panel goes back to shared memory as the update's A operand
+#pragma unroll
+      for (int r = 0; r < RT; ++r) {
+        const int i = tid + CTA_THREADS * r;
+        if (i < n_pad) {
+#pragma unroll
+          for (int k = 0; k < NB; ++k) P[i * PP + k] = row[r][k];
+        }
       }
       __syncthreads();
+      pc->mark(PH_INV_PANEL);
+
+      // ---- apply the panel to the block's other columns, one 64-wide tile at a time
+      auto load_r = [&](cplx* R, int c0) {
+        for (int e = tid; e < NB * GT_N; e += CTA_THREADS) {
+          int kk = e / GT_N, cc = e % GT_N;
+          bool v = (kk < w && c0 + cc < c_hi);
+          const cplx* src = v ? W + (int64_t)piv[p0 + kk] * ldw + c0 + cc : W;
+          cp_async16(R + kk * RP + cc, src, v);
+        }
+        cp_async_commit();
+      };
+      int tiles[INV_OB / GT_N + 1];
+      int ntile = 0;
+      for (int c0 = c_lo; c0 < c_hi; c0 += GT_N) {
+        const int c1 = min(c0 + GT_N, c_hi);
+        if (!(c0 >= p0 && c1 <= p0 + w)) tiles[ntile++] = c0;
+      }
+      if (ntile > 0) load_r(Rb[0], tiles[0]);
+      for (int t = 0; t < ntile; ++t) {
+        const int c0 = tiles[t];
+        cplx* R = Rb[t & 1];
+        if (t + 1 < ntile) load_r(Rb[(t + 1) & 1], tiles[t + 1]);
+        else cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        for (int r0 = 0; r0 < n; r0 += GT_M) {
+          // fetch this warp's slice of W (the addend) ahead of the tensor-core work
+          cplx old[4][2][2];
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+#pragma unroll
+              for (int e = 0; e < 2; ++e) {
+                int row = r0 + wm + i * 8 + gr, col = c0 + wn + j * 8 + 2 * gc + e;
+                old[i][j][e] = cmk(0.0, 0.0);
+                if (row < n && col < c_hi) old[i][j][e] = ldg_early(W + (int64_t)row * ldw + col);
+              }
+          Acc3M acc;
+          acc.zero();
+          warp_mma_3m<false, false>(acc, P + (size_t)r0 * PP, R, NB / 4, wm, wn, lane, PanelIdx{PP}, RIdx());
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+#pragma unroll
+              for (int e = 0; e < 2; ++e) {
+                int row = r0 + wm + i * 8 + gr, col = c0 + wn + j * 8 + 2 * gc + e;
+                if (row < n && col < c_hi && (col < p0 || col >= p0 + w)) {
+                  double t1 = acc.t1[i][j][e], t2 = acc.t2[i][j][e], t3 = acc.t3[i][j][e];
+                  cplx v = cmk(t1 - t2, t3 - t1 - t2);
+                  int lc = pinv[row];
+                  bool is_piv = (lc >= p0 && lc < p0 + w);
+                  W[(int64_t)row * ldw + col] = is_piv ? v : cadd(old[i][j][e], v);
+                }
+              }
+        }
+        __syncthreads();  // R[t & 1] is refilled two tiles later
+      }
+      cp_async_wait<0>();
+      // ---- write the factorised panel back
+      for (int e = tid; e < n * NB; e += CTA_THREADS) {
+        int i = e / NB, jj = e % NB;
+        if (jj < w) W[(int64_t)i * ldw + p0 + jj] = P[i * PP + jj];
+      }
+      __syncthreads();
+      pc->mark(PH_INV_UPDATE);
     }
 
-    // ---- apply the panel to every other column, one 64-wide column tile at a time
-    const int wm = (warp >> 2) * 32, wn = (warp & 3) * 16;
-    for (int c0 = 0; c0 < n; c0 += GT_N) {
-      const int c1 = min(c0 + GT_N, n);
-      if (c0 >= p0 && c1 <= p0 + w) continue;  // tile lies inside the panel
-      for (int e = tid; e < NB * GT_N; e += CTA_THREADS) {
-        int kk = e / GT_N, cc = e % GT_N;
-        cplx v = cmk(0.0, 0.0);
-        if (kk < w && c0 + cc < n) v = W[(int64_t)piv[p0 + kk] * ldw + c0 + cc];
-        R[kk * RP + cc] = v;
+    // ---- apply the block transform to the columns outside the block (k = block width)
+    if (ob < n) {
+      const int kb = c_hi - c_lo;
+#pragma unroll 4
+      for (int e = tid; e < kb * n; e += CTA_THREADS) {
+        int kk = e / n, c = e % n;
+        snap[e] = W[(int64_t)piv[c_lo + kk] * ldw + c];
       }
       __syncthreads();
-      for (int r0 = 0; r0 < n; r0 += GT_M) {
-        Acc3M acc;
-        acc.zero();
-        warp_mma_3m<false, false>(acc, P + (size_t)r0 * PP, R, NB / 4, wm, wn, lane, PanelIdx{PP}, RIdx());
-        acc_foreach(acc, wm, wn, lane, [&](int r, int cc, cplx v) {
-          int i = r0 + r, col = c0 + cc;
-          if (i < n && col < n && (col < p0 || col >= p0 + w)) {
-            int lc = pinv[i];
-            bool is_piv = (lc >= p0 && lc < p0 + w);
-            cplx* dst = W + (int64_t)i * ldw + col;
-            *dst = is_piv ? v : cadd(*dst, v);
-          }
-        });
+      if (c_lo > 0) {
+        GemmArgs g = gemm_args(n, c_lo, kb, W + c_lo, ldw, snap, n, W, ldw);
+        cta_gemm_epi<OP_N, OP_N>(g, reinterpret_cast<cplx*>(smem_raw), EpiGJ{W, ldw, pinv, c_lo, c_hi, 0});
       }
-      __syncthreads();
+      if (c_hi < n) {
+        GemmArgs g = gemm_args(n, n - c_hi, kb, W + c_lo, ldw, snap + c_hi, n, W + c_hi, ldw);
+        cta_gemm_epi<OP_N, OP_N>(g, reinterpret_cast<cplx*>(smem_raw), EpiGJ{W, ldw, pinv, c_lo, c_hi, c_hi});
+      }
+      pc->mark(PH_INV_UPDATE);
     }
-    // ---- write the factorised panel back
-    for (int e = tid; e < n * NB; e += CTA_THREADS) {
-      int i = e / NB, jj = e % NB;
-      if (jj < w) W[(int64_t)i * ldw + p0 + jj] = P[i * PP + jj];
-    }
-    __syncthreads();
   }
 
   // ---- undo the implicit pivoting while storing: G[i][j] = W[p(i)][p^-1(j)]
+#pragma unroll 4
   for (int e = tid; e < n * n; e += CTA_THREADS) {
     int i = e / n, j = e % n;
     G[(int64_t)i * ldg + j] = W[(int64_t)piv[i] * ldw + pinv[j]];
   }
   const int flag = s_misc[1];
   __syncthreads();
+  pc->mark(PH_INV_GATHER);
   return flag;
 }
 
-// Shared-memory bytes cta_inverse needs for an n x n matrix.
-NEGF_DEV size_t inv_smem_bytes(int n) {
-  return n <= 256 ? InvLayout<32>::bytes(n) : InvLayout<16>::bytes(n);
-}
-
-NEGF_DEV int cta_inverse(cplx* W, int64_t ldw, int n, cplx* G, int64_t ldg, char* smem_raw) {
-  if (n <= 256) return cta_inverse_nb<32>(W, ldw, n, G, ldg, smem_raw);
-  return cta_inverse_nb<16>(W, ldw, n, G, ldg, smem_raw);
+NEGF_DEV int cta_inverse(cplx* W, int64_t ldw, int n, cplx* G, int64_t ldg, char* smem_raw, PhaseClock* pc,
+                         cplx* snap) {
+  if (n <= 256) return cta_inverse_nb<32, 1>(W, ldw, n, G, ldg, smem_raw, pc, snap);
+  return cta_inverse_nb<16, 2>(W, ldw, n, G, ldg, smem_raw, pc, snap);
 }
 
 }  // namespace negf

@@ -44,6 +44,13 @@ NEGF_DEV void cp_async16(void* smem_dst, const void* gmem_src, bool valid) {
   int n = valid ? 16 : 0;
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem_src), "r"(n));
 }
+// Global load that the compiler may not sink below later volatile asm (the
+// DMMAs): used to put a read-modify-write's reads in flight before the math.
+NEGF_DEV cplx ldg_early(const cplx* p) {
+  cplx v;
+  asm volatile("ld.global.cg.v2.f64 {%0,%1}, [%2];\n" : "=d"(v.x), "=d"(v.y) : "l"(p));
+  return v;
+}
 NEGF_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 NEGF_DEV void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
@@ -60,5 +67,29 @@ NEGF_DEV void dmma884(double& c0, double& c1, double a, double b) {
 
 // Operand transforms for the tile GEMM.
 enum Op : int { OP_N = 0, OP_C = 1 /* conjugate transpose */, OP_K = 2 /* conjugate */ };
+
+// Per-CTA phase clocks (thread 0): the cycles since the previous mark are
+// charged to the phase that just ended.  Every mark follows a __syncthreads.
+enum Phase {
+  PH_FORM = 0, PH_GEMM_FWD, PH_INV_STAGE, PH_INV_PANEL, PH_INV_UPDATE, PH_INV_GATHER,
+  PH_GEMM_BWD, PH_LESSER, PH_DOS, PH_TRANS, PH_OTHER, NPH
+};
+struct PhaseClock {
+  unsigned long long c[NPH];
+  long long t0;
+  bool on;
+  NEGF_DEV void start(bool enable) {
+    on = enable && threadIdx.x == 0;
+    for (int i = 0; i < NPH; ++i) c[i] = 0;
+    t0 = on ? clock64() : 0;
+  }
+  NEGF_DEV void mark(int ph) {
+    if (on) {
+      long long t = clock64();
+      c[ph] += (unsigned long long)(t - t0);
+      t0 = t;
+    }
+  }
+};
 
 }  // namespace negf

@@ -24,6 +24,7 @@
 #include <cstdio>
 #include "../../include/negf_b200.h"
 #include "cta_inverse.cuh"
+#include "cta_stream.cuh"
 
 namespace negf {
 
@@ -62,47 +63,46 @@ NEGF_DEV SlotBufs slot_bufs(const NegfRgfProblem& p, int slot) {
 }
 
 // Out = X - z Y  ([m x n]); a missing X or Y (offset -1) is a zero block.
-NEGF_DEV void form_shift(cplx* out, const cplx* hs, int64_t ox, int64_t oy, cplx z, int m, int n) {
-  const int tid = threadIdx.x;
-  for (int e = tid; e < m * n; e += CTA_THREADS) {
-    cplx x = ox >= 0 ? hs[ox + e] : cmk(0.0, 0.0);
-    cplx y = oy >= 0 ? hs[oy + e] : cmk(0.0, 0.0);
-    out[e] = csub(x, cmul(z, y));
-  }
+NEGF_DEV void form_shift(cplx* out, const cplx* hs, int64_t ox, int64_t oy, cplx z, int m, int n, cplx* smem) {
+  cta_shift_form(out, ox >= 0 ? hs + ox : nullptr, oy >= 0 ? hs + oy : nullptr, z, cmk(1.0, 0.0), m * n, smem);
 }
 
 // W = z S - H - (Sigma_L in the top-left corner) - (Sigma_R in the bottom-right
 // corner); the corner rule is recursive_green_cal.py:411-428.
 NEGF_DEV void form_a0(cplx* W, const cplx* hs, const NegfBlock& b, cplx z, const cplx* seL, int nsl,
-                      const cplx* seR, int nsr) {
+                      const cplx* seR, int nsr, cplx* smem) {
   const int n = b.n, tid = threadIdx.x;
+  cta_shift_form(W, hs + b.hd, hs + b.sd, z, cmk(-1.0, 0.0), n * n, smem);
   const int cl = seL ? min(n, nsl) : 0;
   const int cr = seR ? min(n, nsr) : 0;
-  for (int e = tid; e < n * n; e += CTA_THREADS) {
-    int i = e / n, j = e % n;
-    cplx v = csub(cmul(z, hs[b.sd + e]), hs[b.hd + e]);
-    if (i < cl && j < cl) v = csub(v, seL[(int64_t)i * nsl + j]);
-    if (i >= n - cr && j >= n - cr) {
-      int ii = i - (n - cr) + (nsr - cr), jj = j - (n - cr) + (nsr - cr);
-      v = csub(v, seR[(int64_t)ii * nsr + jj]);
-    }
-    W[e] = v;
+  for (int e = tid; e < cl * cl; e += CTA_THREADS) {
+    int i = e / cl, j = e % cl;
+    W[(int64_t)i * n + j] = csub(W[(int64_t)i * n + j], seL[(int64_t)i * nsl + j]);
   }
+  __syncthreads();  // a block can carry both corners (K = 1)
+  for (int e = tid; e < cr * cr; e += CTA_THREADS) {
+    int i = e / cr, j = e % cr;
+    int64_t w = (int64_t)(n - cr + i) * n + (n - cr + j);
+    W[w] = csub(W[w], seR[(int64_t)(nsr - cr + i) * nsr + (nsr - cr + j)]);
+  }
+  __syncthreads();
 }
 
-NEGF_DEV void copy_mat(cplx* dst, const cplx* src, int m, int n) {
-  for (int e = threadIdx.x; e < m * n; e += CTA_THREADS) dst[e] = src[e];
+NEGF_DEV void copy_mat(cplx* dst, const cplx* src, int m, int n, cplx* smem) {
+  cta_shift_form(dst, src, nullptr, cmk(0.0, 0.0), cmk(1.0, 0.0), m * n, smem);
 }
 
-// dst[i] (+)= -Im( sum_j A[i][j] B[j][i] ) / pi   (A: rows x inner, B: inner x rows).
-// dst may be null; the row values are also summed into dsum (lane 0 of each warp).
-NEGF_DEV void diag_im_acc(double* dst, double& dsum, const cplx* A, const cplx* B, int rows, int inner,
+// dst[i] (+)= -Im( sum_j A[i][j] BT[i][j] ) / pi  = -Im diag(A B)_i / pi, with
+// BT = B^T stored row-major (A and BT both rows x inner).  dst may be null;
+// the row values are also summed into dsum (lane 0 of each warp).
+NEGF_DEV void diag_im_acc(double* dst, double& dsum, const cplx* A, const cplx* BT, int rows, int inner,
                           bool init) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int i = warp; i < rows; i += CTA_THREADS / 32) {
     double acc = 0.0;
+#pragma unroll 4
     for (int j = lane; j < inner; j += 32) {
-      cplx a = A[(int64_t)i * inner + j], b = B[(int64_t)j * rows + i];
+      cplx a = A[(int64_t)i * inner + j], b = BT[(int64_t)i * inner + j];
       acc += a.x * b.y + a.y * b.x;
     }
 #pragma unroll
@@ -114,27 +114,6 @@ NEGF_DEV void diag_im_acc(double* dst, double& dsum, const cplx* A, const cplx* 
     }
   }
 }
-
-// Per-CTA phase clocks (thread 0): the cycles since the previous mark are
-// charged to the phase that just ended.  Every mark follows a __syncthreads.
-enum Phase { PH_FORM = 0, PH_GEMM_FWD, PH_INV, PH_GEMM_BWD, PH_LESSER, PH_DOS, PH_TRANS, PH_OTHER, NPH };
-struct PhaseClock {
-  unsigned long long c[NPH];
-  long long t0;
-  bool on;
-  NEGF_DEV void start(bool enable) {
-    on = enable && threadIdx.x == 0;
-    for (int i = 0; i < NPH; ++i) c[i] = 0;
-    t0 = on ? clock64() : 0;
-  }
-  NEGF_DEV void mark(int ph) {
-    if (on) {
-      long long t = clock64();
-      c[ph] += (unsigned long long)(t - t0);
-      t0 = t;
-    }
-  }
-};
 
 // Gamma = i (Sigma - Sigma^H) on the c x c corner of Sigma (ns x ns) at (r0, r0).
 NEGF_DEV void form_gamma(cplx* out, const cplx* se, int ns, int r0, int c) {
@@ -202,12 +181,12 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
   for (int q = 0; q < K; ++q) {
     const NegfBlock& b = blk[q];
     const int nq = b.n;
-    form_a0(sb.W, hs, b, z, q == 0 ? seL : nullptr, it.nse_l, q == K - 1 ? seR : nullptr, it.nse_r);
+    form_a0(sb.W, hs, b, z, q == 0 ? seL : nullptr, it.nse_l, q == K - 1 ? seR : nullptr, it.nse_r, smem);
     if (q > 0) {
       const NegfBlock& bp = blk[q - 1];
       const int np = bp.n;
-      form_shift(sb.Lz, hs, bp.hl, bp.sl, z, nq, np);  // L_{q-1}: n_q x n_{q-1}
-      form_shift(sb.Uz, hs, bp.hu, bp.su, z, np, nq);  // U_{q-1}: n_{q-1} x n_q
+      form_shift(sb.Lz, hs, bp.hl, bp.sl, z, nq, np, smem);  // L_{q-1}: n_q x n_{q-1}
+      form_shift(sb.Uz, hs, bp.hu, bp.su, z, np, nq, smem);  // U_{q-1}: n_{q-1} x n_q
       __syncthreads();
       pc.mark(PH_FORM);
       gemm<OP_N, OP_N>(smem, nq, np, np, sb.Lz, np, gptr(q - 1), np, sb.T1, np);
@@ -217,8 +196,7 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
       __syncthreads();
       pc.mark(PH_FORM);
     }
-    bad |= cta_inverse(sb.W, nq, nq, gptr(q), nq, smem_raw);
-    pc.mark(PH_INV);
+    bad |= cta_inverse(sb.W, nq, nq, gptr(q), nq, smem_raw, &pc, sb.tE);  // tE: pivot-row snapshot
     if (lesser) {
       // gin_q = g_q (s_q + L gin_{q-1} U) g_q^H
       const cplx* s = sinptr(q);
@@ -228,7 +206,7 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
         if (s) gemm<OP_N, OP_N>(smem, nq, nq, np, sb.T1, np, sb.Uz, nq, sb.tA, nq, ONE, s, nq);
         else gemm<OP_N, OP_N>(smem, nq, nq, np, sb.T1, np, sb.Uz, nq, sb.tA, nq);
       } else {
-        if (s) copy_mat(sb.tA, s, nq, nq);
+        if (s) copy_mat(sb.tA, s, nq, nq, smem);
         else for (int e = threadIdx.x; e < nq * nq; e += CTA_THREADS) sb.tA[e] = cmk(0.0, 0.0);
         __syncthreads();
       }
@@ -248,13 +226,13 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
   const cplx* Gnext = gptr(K - 1);
   if (fl & NEGF_OUT_GRD) {
     cplx* d = out + blk[K - 1].o_grd + row * sq(K - 1);
-    copy_mat(d, gptr(K - 1), nN, nN);
+    copy_mat(d, gptr(K - 1), nN, nN, smem);
     Gnext = d;
   }
   const cplx* gt = gptr(K - 1);
   if (fl & NEGF_OUT_GR_LC) {
     cplx* d = out + blk[K - 1].o_grlc + row * sq(K - 1);
-    copy_mat(d, gptr(K - 1), nN, nN);
+    copy_mat(d, gptr(K - 1), nN, nN, smem);
     gt = d;
   }
   const cplx* Nnext = nullptr;  // gnd_{q+1}
@@ -262,14 +240,14 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
     Nnext = ginptr(K - 1);
     if (blk[K - 1].o_gnd >= 0) {
       cplx* d = out + blk[K - 1].o_gnd + row * sq(K - 1);
-      copy_mat(d, ginptr(K - 1), nN, nN);
+      copy_mat(d, ginptr(K - 1), nN, nN, smem);
       Nnext = d;
     }
   }
   __syncthreads();
   pc.mark(PH_FORM);
   if (want_dos) {
-    diag_im_acc(orb ? orb + blk[K - 1].orb0 : nullptr, dsum, gptr(K - 1), hs + blk[K - 1].sd, nN, nN, true);
+    diag_im_acc(orb ? orb + blk[K - 1].orb0 : nullptr, dsum, gptr(K - 1), hs + blk[K - 1].sdT, nN, nN, true);
     __syncthreads();
     pc.mark(PH_DOS);
   }
@@ -278,8 +256,8 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
     const NegfBlock& b = blk[q];
     const int nq = b.n, nn = b.n_next;
     const int64_t szu = (int64_t)nq * nn;
-    form_shift(sb.Lz, hs, b.hl, b.sl, z, nn, nq);  // L_q: n_{q+1} x n_q
-    form_shift(sb.Uz, hs, b.hu, b.su, z, nq, nn);  // U_q: n_q x n_{q+1}
+    form_shift(sb.Lz, hs, b.hl, b.sl, z, nn, nq, smem);  // L_q: n_{q+1} x n_q
+    form_shift(sb.Uz, hs, b.hu, b.su, z, nq, nn, smem);  // U_q: n_q x n_{q+1}
     __syncthreads();
     pc.mark(PH_FORM);
     const cplx* g = gptr(q);
@@ -325,14 +303,14 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
       pc.mark(PH_LESSER);
     }
     if (want_dos) {
-      diag_im_acc(orb ? orb + b.orb0 : nullptr, dsum, grd, hs + b.sd, nq, nq, true);
+      diag_im_acc(orb ? orb + b.orb0 : nullptr, dsum, grd, hs + b.sdT, nq, nq, true);
       __syncthreads();
-      if (b.sl >= 0) {
-        diag_im_acc(orb ? orb + b.orb0 : nullptr, dsum, gru, hs + b.sl, nq, nn, false);
+      if (b.slT >= 0) {
+        diag_im_acc(orb ? orb + b.orb0 : nullptr, dsum, gru, hs + b.slT, nq, nn, false);
         __syncthreads();
       }
-      if (b.su >= 0) {
-        diag_im_acc(orb ? orb + blk[q + 1].orb0 : nullptr, dsum, grl, hs + b.su, nn, nq, false);
+      if (b.suT >= 0) {
+        diag_im_acc(orb ? orb + blk[q + 1].orb0 : nullptr, dsum, grl, hs + b.suT, nn, nq, false);
         __syncthreads();
       }
       pc.mark(PH_DOS);
@@ -341,7 +319,7 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
   }
   if (fl & NEGF_OUT_GTRANS) {
     cplx* d = out + dv.o_gtrans + row * (int64_t)blk[0].n * nN;
-    copy_mat(d, gt, blk[0].n, nN);
+    copy_mat(d, gt, blk[0].n, nN, smem);
     __syncthreads();
   }
   double dos_total = 0.0;
@@ -401,10 +379,14 @@ __global__ void __launch_bounds__(CTA_THREADS, 1) rgf_kernel(const NegfRgfProble
     for (int i = 0; i < NPH; ++i) P.phase_cycles[(size_t)blockIdx.x * NPH + i] = pc.c[i];
 }
 
+// Dynamic shared memory: the union of the GEMM ring, the inverse panel and the
+// streaming buffers (they are used one after another).
 size_t rgf_smem_bytes(int max_n) {
-  size_t a = GEMM_SMEM_BYTES, b = inv_smem_bytes_host(max_n);
-  return a > b ? a : b;
+  size_t a = GEMM_SMEM_BYTES, b = inv_smem_bytes_host(max_n), c = STREAM_SMEM_BYTES;
+  size_t m = a > b ? a : b;
+  return m > c ? m : c;
 }
+static_assert(CTA_THREADS == 256, "cta_stream.cuh assumes 256-thread CTAs");
 
 }  // namespace negf
 

@@ -75,7 +75,8 @@ class Geometry:
                 b["n_next"] = dims[q + 1] if q + 1 < K else 0
                 b["hd"] = put(d.hd[q])
                 b["sd"] = put(d.sd[q])
-                for name in ("hu", "su", "hl", "sl"):
+                b["sdT"] = put(d.sd[q].mT)
+                for name in ("hu", "su", "hl", "sl", "suT", "slT"):
                     b[name] = -1
                 if q + 1 < K:
                     nn = dims[q + 1]
@@ -84,6 +85,9 @@ class Geometry:
                         t = lst[q]
                         if tuple(t.shape[-2:]) != shape:
                             raise ValueError(f"{name}[{q}] has shape {tuple(t.shape)}, expected {shape}")
+                        b[name] = put(t)
+                        offdiag.append((len(blocks), name, int(b[name]), t.numel()))
+                    for name, t in (("suT", d.su[q].mT), ("slT", d.sl[q].mT)):
                         b[name] = put(t)
                         offdiag.append((len(blocks), name, int(b[name]), t.numel()))
                 b["orb0"] = orb

@@ -56,7 +56,8 @@ extern "C" {
 #define NEGF_DOS (1u << 9)         /* DOS = 2 sum_i (-Im diag(G S)_i / pi) -> dos[]  */
 
 /* Phase indices of NegfRgfProblem.phase_cycles (clock64 cycles per slot). */
-#define NEGF_PHASES 8 /* form, gemm_fwd, inverse, gemm_bwd, lesser, dos, trans, other */
+#define NEGF_PHASES 11 /* form, gemm_fwd, inv_stage, inv_panel, inv_update, inv_gather,
+                          gemm_bwd, lesser, dos, trans, other */
 
 /* One diagonal block q of a block-tridiagonal device. */
 typedef struct NegfBlock {
@@ -65,6 +66,8 @@ typedef struct NegfBlock {
   int64_t hd, sd; /* offsets of H_qq, S_qq in hs */
   int64_t hu, su; /* offsets of H_{q,q+1}, S_{q,q+1} [n_q x n_{q+1}]; -1 = zero block */
   int64_t hl, sl; /* offsets of H_{q+1,q}, S_{q+1,q} [n_{q+1} x n_q]; -1 = zero block */
+  int64_t sdT, suT, slT; /* transposed copies S_qq^T, S_{q,q+1}^T, S_{q+1,q}^T (row-major) used by
+                            the DOS diagonals; -1 = zero block */
   int64_t orb0;   /* first orbital of block q within its device */
   int64_t g;      /* offset of g_q inside one item's g slab (prefix sum of n^2) */
   /* block outputs: offset of batch row 0 in out; row b adds b * (block size).

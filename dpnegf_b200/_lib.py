@@ -49,6 +49,30 @@ ITEM_DTYPE = np.dtype([("dev", "<i4"), ("row", "<i4"), ("z_re", "<f8"), ("z_im",
                        ("out", "<i8"), ("orb", "<i8")])
 
 
+LEAD_DTYPE = np.dtype([("n", "<i4"), ("nc", "<i4"), ("b", "<i4"), ("pad", "<i4"), ("h", "<i8"), ("s", "<i8"),
+                       ("h01", "<i8"), ("s01", "<i8"), ("hdl", "<i8"), ("sdl", "<i8")])
+LS_ITEM_DTYPE = np.dtype([("lead", "<i4"), ("pad", "<i4"), ("e_re", "<f8"), ("e_im", "<f8"), ("eta", "<f8"),
+                          ("sigma", "<u8"), ("gs", "<u8"), ("out", "<i8")])
+
+
+class NegfLsProblem(ctypes.Structure):
+    _fields_ = [
+        ("leads", ctypes.c_void_p),
+        ("items", ctypes.c_void_p),
+        ("n_items", ctypes.c_int32),
+        ("max_n", ctypes.c_int32),
+        ("arena", ctypes.c_void_p),
+        ("status", ctypes.c_void_p),
+        ("iters", ctypes.c_void_p),
+        ("resid", ctypes.c_void_p),
+        ("tol", ctypes.c_double),
+        ("max_iter", ctypes.c_int32),
+        ("n_slots", ctypes.c_int32),
+        ("scratch", ctypes.c_void_p),
+        ("scratch_bytes", ctypes.c_size_t),
+    ]
+
+
 class NegfRgfProblem(ctypes.Structure):
     _fields_ = [
         ("blocks", ctypes.c_void_p),
@@ -97,6 +121,10 @@ def load():
     lib.negf_version.restype = ctypes.c_char_p
     lib.negf_abi_struct_size.restype = ctypes.c_size_t
     lib.negf_abi_struct_size.argtypes = [ctypes.c_int]
+    lib.negf_lopez_sancho_scratch_bytes.restype = ctypes.c_size_t
+    lib.negf_lopez_sancho_scratch_bytes.argtypes = [ctypes.POINTER(NegfLsProblem)]
+    lib.negf_lopez_sancho_run.restype = ctypes.c_int
+    lib.negf_lopez_sancho_run.argtypes = [ctypes.POINTER(NegfLsProblem), ctypes.c_void_p]
     _lib = lib
     return lib
 

@@ -1,0 +1,262 @@
+// Batched Lopez-Sancho decimation for lead surface Green's functions and
+// self-energies (sm_100a, FP64 tensor cores).
+//
+// Persistent kernel: one CTA per work slot pulls (lead, energy) items from an
+// atomic queue and runs the whole decimation for that item in a private
+// scratch slot, with the same CTA tile GEMM and blocked Gauss-Jordan inverse
+// as the RGF sweep.  Follows _surface_green_numba_core
+// (negf/surface_green.py:102-159) step for step:
+//   alpha = h10 - z s10,  beta = h01 - z s01,  eps = eps_s = H
+//   repeat (at most max_iter + 1 times):
+//     Xa = (zS - eps)^-1 alpha,  Xb = (zS - eps)^-1 beta
+//     eps += alpha Xb + beta Xa;  eps_s += beta Xa
+//     alpha <- alpha Xa;  beta <- beta Xb
+//     stop when max(|alpha| + |beta|) < tol
+//   g_s = (zS - eps_s)^-1, accepted when
+//     max |(zS - H - (z s01 - h01) g_s (z s10 - h10)) g_s - I| < 3e-5
+//     (warning status above 1e-8)
+// and the self-energy product of selfEnergy (:73-86):
+//   Sigma = (E S_DL - H_DL) g_s[:b,:b] (E S_DL^H - H_DL^H),   E without i*eta,
+// or the bulk form Sigma = (E S - H) - g_s^-1 when the lead has no H_DL.
+#include <cstdio>
+#include "../../include/negf_b200.h"
+#include "cta_inverse.cuh"
+#include "cta_stream.cuh"
+
+namespace negf {
+
+constexpr int LS_NBUF = 14;  // max_n^2 buffers per slot (see ls_item)
+constexpr size_t LS_SCRATCH_HEADER = 256;
+
+__host__ __device__ inline size_t ls_slot_elems(const NegfLsProblem& p) {
+  size_t mn2 = (size_t)p.max_n * p.max_n;
+  size_t e = LS_NBUF * mn2 + inv_snapshot_elems(p.max_n);
+  return (e + 15) & ~(size_t)15;
+}
+
+// out[i][j] = conj(X[j][i]) - z conj(Y[j][i])   (n x n), i.e. X^H - z Y^H
+NEGF_DEV void form_herm_shift(cplx* out, const cplx* X, const cplx* Y, cplx z, int n) {
+#pragma unroll 4
+  for (int e = threadIdx.x; e < n * n; e += CTA_THREADS) {
+    int i = e / n, j = e % n;
+    cplx x = cconj(X[(int64_t)j * n + i]), y = cconj(Y[(int64_t)j * n + i]);
+    out[e] = csub(x, cmul(z, y));
+  }
+  __syncthreads();
+}
+
+// out[i][j] = z conj(S[j][i]) - conj(H[j][i])   for an (rows x cols) H/S pair
+// stored (cols x rows): E S^H - H^H.
+NEGF_DEV void form_eS_minus_h_herm(cplx* out, const cplx* H, const cplx* S, cplx z, int rows, int cols) {
+  for (int e = threadIdx.x; e < rows * cols; e += CTA_THREADS) {
+    int i = e / cols, j = e % cols;
+    cplx h = cconj(H[(int64_t)j * rows + i]), s = cconj(S[(int64_t)j * rows + i]);
+    out[e] = csub(cmul(z, s), h);
+  }
+  __syncthreads();
+}
+
+NEGF_DEV double cta_max(double v, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double m = red[0];
+  for (int w = 1; w < CTA_THREADS / 32; ++w) m = fmax(m, red[w]);
+  __syncthreads();
+  return m;
+}
+
+template <int OPA, int OPB>
+NEGF_DEV void gemm_ls(cplx* smem, int M, int N, int K, const cplx* A, int64_t lda, const cplx* B, int64_t ldb,
+                      cplx* C, int64_t ldc, const cplx* D = nullptr, int64_t ldd = 0,
+                      cplx alpha = cmk(1.0, 0.0), cplx beta = cmk(1.0, 0.0)) {
+  GemmArgs g = gemm_args(M, N, K, A, lda, B, ldb, C, ldc);
+  g.alpha = alpha;
+  if (D) { g.D = D; g.ldd = ldd; g.beta = beta; g.use_d = true; }
+  cta_gemm<OPA, OPB>(g, smem);
+}
+
+NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, char* smem_raw, double* red) {
+  cplx* smem = reinterpret_cast<cplx*>(smem_raw);
+  const NegfLead ld = P.leads[it.lead];
+  const int n = ld.n;
+  const int64_t n2 = (int64_t)n * n;
+  const size_t mn2 = (size_t)P.max_n * P.max_n;
+  const cplx* ar = reinterpret_cast<const cplx*>(P.arena);
+  const cplx* H = ar + ld.h;
+  const cplx* S = ar + ld.s;
+  const cplx* h01 = ar + ld.h01;
+  const cplx* s01 = ar + ld.s01;
+  const cplx E = cmk(it.e_re, it.e_im);
+  const cplx z = cmk(it.e_re, it.e_im + it.eta);
+  const cplx ONE = cmk(1.0, 0.0);
+  PhaseClock pc;
+  pc.start(false);
+  cplx* b_[LS_NBUF];
+  for (int i = 0; i < LS_NBUF; ++i) b_[i] = slot + i * mn2;
+  cplx *eps = b_[0], *epss = b_[1], *alpha = b_[2], *beta = b_[3], *alpha2 = b_[4], *beta2 = b_[5];
+  cplx *A = b_[6], *Ainv = b_[7], *Xa = b_[8], *Xb = b_[9], *T = b_[10], *gsb = b_[11], *t1 = b_[12],
+       *t2 = b_[13];
+  cplx* snap = slot + LS_NBUF * mn2;
+  int bad = 0;
+
+  // alpha = h10 - z s10 = h01^H - z s01^H ; beta = h01 - z s01 ; eps = eps_s = H
+  form_herm_shift(alpha, h01, s01, z, n);
+  cta_shift_form(beta, h01, s01, z, ONE, (int)n2, smem);
+  cta_shift_form(eps, H, nullptr, cmk(0.0, 0.0), ONE, (int)n2, smem);
+  cta_shift_form(epss, H, nullptr, cmk(0.0, 0.0), ONE, (int)n2, smem);
+
+  int it_n = 0;
+  bool converged = false;
+  for (int iter = 1; iter <= P.max_iter + 1; ++iter) {
+    it_n = iter;
+    // A = zS - eps
+    cta_shift_form(A, eps, S, z, cmk(-1.0, 0.0), (int)n2, smem);
+    bad |= cta_inverse(A, n, n, Ainv, n, smem_raw, &pc, snap);
+    gemm_ls<OP_N, OP_N>(smem, n, n, n, Ainv, n, alpha, n, Xa, n);
+    gemm_ls<OP_N, OP_N>(smem, n, n, n, Ainv, n, beta, n, Xb, n);
+    gemm_ls<OP_N, OP_N>(smem, n, n, n, beta, n, Xa, n, T, n);  // beta Xa
+    // eps_s += beta Xa ; eps += beta Xa (then + alpha Xb below)
+#pragma unroll 4
+    for (int e = threadIdx.x; e < n2; e += CTA_THREADS) {
+      epss[e] = cadd(epss[e], T[e]);
+      eps[e] = cadd(eps[e], T[e]);
+    }
+    __syncthreads();
+    gemm_ls<OP_N, OP_N>(smem, n, n, n, alpha, n, Xb, n, eps, n, eps, n);  // eps += alpha Xb
+    gemm_ls<OP_N, OP_N>(smem, n, n, n, alpha, n, Xa, n, alpha2, n);        // alpha <- alpha Xa
+    gemm_ls<OP_N, OP_N>(smem, n, n, n, beta, n, Xb, n, beta2, n);          // beta <- beta Xb
+    cplx* t = alpha; alpha = alpha2; alpha2 = t;
+    t = beta; beta = beta2; beta2 = t;
+    double m = 0.0;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < n2; e += CTA_THREADS) {
+      cplx a = alpha[e], b = beta[e];
+      double v = hypot(a.x, a.y) + hypot(b.x, b.y);
+      m = (v == v) ? fmax(m, v) : INFINITY;
+    }
+    m = cta_max(m, red);
+    if (m < P.tol) { converged = true; break; }
+    if (!isfinite(m)) break;
+  }
+
+  int st = NEGF_OK;
+  double res = INFINITY;
+  if (!converged) {
+    st = NEGF_ERR_LS_NOT_CONVERGED;
+  } else {
+    cplx* gs = it.gs ? reinterpret_cast<cplx*>(it.gs) : gsb;
+    // g_s = (zS - eps_s)^-1
+    cta_shift_form(A, epss, S, z, cmk(-1.0, 0.0), (int)n2, smem);
+    bad |= cta_inverse(A, n, n, gs, n, smem_raw, &pc, snap);
+    // residual: (zS - H - (z s01 - h01) g_s (z s10 - h10)) g_s - I
+    // z s01 - h01
+#pragma unroll 4
+    for (int e = threadIdx.x; e < n2; e += CTA_THREADS) t1[e] = csub(cmul(z, s01[e]), h01[e]);
+    __syncthreads();
+    // z s10 - h10 = z s01^H - h01^H
+    form_eS_minus_h_herm(t2, h01, s01, z, n, n);
+    gemm_ls<OP_N, OP_N>(smem, n, n, n, t1, n, gs, n, Xa, n);  // (z s01 - h01) g_s
+    gemm_ls<OP_N, OP_N>(smem, n, n, n, Xa, n, t2, n, Xb, n);  // ... (z s10 - h10)
+    // test = zS - H - Xb
+#pragma unroll 4
+    for (int e = threadIdx.x; e < n2; e += CTA_THREADS) T[e] = csub(csub(cmul(z, S[e]), H[e]), Xb[e]);
+    __syncthreads();
+    gemm_ls<OP_N, OP_N>(smem, n, n, n, T, n, gs, n, Xa, n);  // test g_s
+    double m = 0.0;
+    for (int e = threadIdx.x; e < n2; e += CTA_THREADS) {
+      cplx v = Xa[e];
+      if (e / n == e % n) v.x -= 1.0;
+      double a = hypot(v.x, v.y);
+      m = (a == a) ? fmax(m, a) : INFINITY;
+    }
+    res = cta_max(m, red);
+    if (!(res < 3.0e-5)) st = NEGF_ERR_LS_RESIDUAL;
+    else if (res > 1.0e-8) st = NEGF_WARN_LS_CONVERGENCE;
+
+    if (it.sigma && st != NEGF_ERR_LS_RESIDUAL) {
+      cplx* sig = reinterpret_cast<cplx*>(it.sigma);
+      if (ld.nc > 0) {
+        const int nc = ld.nc, b = ld.b;
+        const cplx* hdl = ar + ld.hdl;
+        const cplx* sdl = ar + ld.sdl;
+        // t1 = E S_DL - H_DL  (nc x b)
+        for (int e = threadIdx.x; e < nc * b; e += CTA_THREADS) t1[e] = csub(cmul(E, sdl[e]), hdl[e]);
+        __syncthreads();
+        // t2 = E S_DL^H - H_DL^H (b x nc)
+        form_eS_minus_h_herm(t2, hdl, sdl, E, b, nc);
+        gemm_ls<OP_N, OP_N>(smem, nc, b, b, t1, b, gs, n, Xa, b);   // (E S_DL - H_DL) g_s[:b,:b]
+        gemm_ls<OP_N, OP_N>(smem, nc, nc, b, Xa, b, t2, nc, sig, nc);
+      } else {
+        // bulk form: Sigma = (E S - H) - g_s^-1
+        cta_shift_form(A, gs, nullptr, cmk(0.0, 0.0), ONE, (int)n2, smem);
+        bad |= cta_inverse(A, n, n, Xa, n, smem_raw, &pc, snap);
+#pragma unroll 4
+        for (int e = threadIdx.x; e < n2; e += CTA_THREADS) sig[e] = csub(csub(cmul(E, S[e]), H[e]), Xa[e]);
+        __syncthreads();
+      }
+    }
+  }
+  if (bad && st == NEGF_OK) st = NEGF_ERR_SINGULAR;
+  if (threadIdx.x == 0) {
+    P.status[it.out] = st;
+    if (P.iters) P.iters[it.out] = it_n;
+    if (P.resid) P.resid[it.out] = res;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(CTA_THREADS, 1) ls_kernel(const NegfLsProblem P) {
+  extern __shared__ __align__(16) char smem[];
+  __shared__ int s_item;
+  __shared__ double red[CTA_THREADS / 32];
+  unsigned* queue = reinterpret_cast<unsigned*>(P.scratch);
+  cplx* slot = reinterpret_cast<cplx*>(reinterpret_cast<char*>(P.scratch) + LS_SCRATCH_HEADER) +
+               (size_t)blockIdx.x * ls_slot_elems(P);
+  for (;;) {
+    if (threadIdx.x == 0) s_item = (int)atomicAdd(queue, 1u);
+    __syncthreads();
+    const int idx = s_item;
+    __syncthreads();
+    if (idx >= P.n_items) break;
+    const NegfLsItem it = P.items[idx];
+    ls_item(P, it, slot, smem, red);
+  }
+}
+
+size_t ls_smem_bytes(int max_n) {
+  size_t a = GEMM_SMEM_BYTES, b = inv_smem_bytes_host(max_n), c = STREAM_SMEM_BYTES;
+  size_t m = a > b ? a : b;
+  return m > c ? m : c;
+}
+
+}  // namespace negf
+
+extern "C" {
+
+size_t negf_lopez_sancho_scratch_bytes(const NegfLsProblem* p) {
+  if (!p || p->n_slots <= 0 || p->max_n <= 0) return 0;
+  return negf::LS_SCRATCH_HEADER + (size_t)p->n_slots * negf::ls_slot_elems(*p) * sizeof(double2);
+}
+
+int negf_lopez_sancho_run(const NegfLsProblem* p, void* stream) {
+  if (!p || !p->leads || !p->items || !p->arena || !p->status || !p->scratch) return NEGF_ERR_ARGUMENT;
+  if (p->n_items <= 0) return NEGF_OK;
+  if (p->max_n <= 0 || p->n_slots <= 0 || p->max_iter < 0) return NEGF_ERR_ARGUMENT;
+  if (p->max_n > NEGF_MAX_BLOCK) return NEGF_ERR_UNSUPPORTED;
+  if (p->scratch_bytes < negf_lopez_sancho_scratch_bytes(p)) return NEGF_ERR_ARGUMENT;
+  if ((reinterpret_cast<uintptr_t>(p->scratch) & 255) != 0) return NEGF_ERR_ARGUMENT;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const size_t smem = negf::ls_smem_bytes(p->max_n);
+  if (cudaFuncSetAttribute(negf::ls_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return NEGF_ERR_CUDA;
+  if (cudaMemsetAsync(p->scratch, 0, negf::LS_SCRATCH_HEADER, s) != cudaSuccess) return NEGF_ERR_CUDA;
+  const int grid = p->n_slots < p->n_items ? p->n_slots : p->n_items;
+  negf::ls_kernel<<<grid, negf::CTA_THREADS, smem, s>>>(*p);
+  return cudaGetLastError() == cudaSuccess ? NEGF_OK : NEGF_ERR_CUDA;
+}
+
+}  // extern "C"

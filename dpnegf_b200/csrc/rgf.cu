@@ -436,6 +436,9 @@ size_t negf_abi_struct_size(int which) {
     case 1: return sizeof(NegfDevice);
     case 2: return sizeof(NegfItem);
     case 3: return sizeof(NegfRgfProblem);
+    case 4: return sizeof(NegfLead);
+    case 5: return sizeof(NegfLsItem);
+    case 6: return sizeof(NegfLsProblem);
     default: return 0;
   }
 }

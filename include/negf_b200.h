@@ -121,6 +121,58 @@ typedef struct NegfRgfProblem {
   unsigned long long* phase_cycles; /* optional [n_slots x NEGF_PHASES] SM-cycle counters; NULL = off */
 } NegfRgfProblem;
 
+/* ---- Lopez-Sancho lead decimation ------------------------------------ */
+
+/* One lead principal layer (energy independent).  Offsets into `arena`. */
+typedef struct NegfLead {
+  int32_t n;   /* principal-layer size */
+  int32_t nc;  /* rows of H_DL (device side of the coupling); 0 = bulk form Sigma = (ES - H) - g_s^-1 */
+  int32_t b;   /* columns of H_DL (leading block of g_s used), <= n */
+  int32_t pad;
+  int64_t h, s, h01, s01; /* H, S, H_01, S_01 [n x n] (H_01 couples the surface layer to the next) */
+  int64_t hdl, sdl;       /* H_DL, S_DL [nc x b]; -1 when nc == 0 */
+} NegfLead;
+
+/* One decimation: a lead at one energy. */
+typedef struct NegfLsItem {
+  int32_t lead;
+  int32_t pad;
+  double e_re, e_im; /* E = energy + E_ref (may be complex, e.g. Ozaki poles) */
+  double eta;        /* decimation runs at z = E + i eta (surface_green.py:65-70, :83) */
+  double* sigma;     /* complex128 [nc x nc] (or [n x n] bulk form) output; NULL = not wanted */
+  double* gs;        /* complex128 [n x n] surface Green's function output; NULL = not wanted */
+  int64_t out;       /* index into status[], iters[], resid[] */
+} NegfLsItem;
+
+typedef struct NegfLsProblem {
+  const NegfLead* leads;    /* device memory */
+  const NegfLsItem* items;  /* device memory */
+  int32_t n_items;
+  int32_t max_n;
+  const double* arena;      /* complex128 lead blocks */
+  int32_t* status;          /* [n_items]: NEGF_OK, NEGF_WARN_LS_CONVERGENCE, NEGF_ERR_LS_* , NEGF_ERR_SINGULAR */
+  int32_t* iters;           /* [n_items] decimation steps taken */
+  double* resid;            /* [n_items] max |(ES - H - (zs01-h01) g_s (zs10-h10)) g_s - I| */
+  double tol;               /* convergence threshold on max(|alpha|+|beta|) (1e-40 in the reference) */
+  int32_t max_iter;         /* 100 in the reference: the step after it raises */
+  int32_t n_slots;
+  void* scratch;
+  size_t scratch_bytes;
+} NegfLsProblem;
+
+/* Bytes of scratch negf_lopez_sancho_run needs for p->n_slots and p->max_n. */
+size_t negf_lopez_sancho_scratch_bytes(const NegfLsProblem* p);
+
+/* Batched Lopez-Sancho decimation over (lead, energy) items, one CTA per item.
+ * Replaces _surface_green_numba_core (negf/surface_green.py:102-159) and the
+ * self-energy product of selfEnergy (:9-91):
+ *   alpha = h10 - z s10, beta = h01 - z s01, eps = eps_s = H;
+ *   [Xa Xb] = (zS - eps)^-1 [alpha beta]; eps += alpha Xb + beta Xa;
+ *   eps_s += beta Xa; alpha <- alpha Xa; beta <- beta Xb
+ * until max(|alpha| + |beta|) < tol; g_s = (zS - eps_s)^-1 with the residual
+ * check of :142-155; Sigma = (E S_DL - H_DL) g_s[:b,:b] (E S_DL^H - H_DL^H). */
+int negf_lopez_sancho_run(const NegfLsProblem* p, void* cuda_stream);
+
 /* Bytes of scratch negf_rgf_run needs for p->n_slots, p->max_n, p->max_g_slab, p->flags. */
 size_t negf_rgf_scratch_bytes(const NegfRgfProblem* p);
 
@@ -158,7 +210,8 @@ int negf_sm_count(void);
 const char* negf_version(void);
 
 /* sizeof of the ABI structs (0 NegfBlock, 1 NegfDevice, 2 NegfItem,
- * 3 NegfRgfProblem) so bindings can verify their mirrors; 0 if unknown. */
+ * 3 NegfRgfProblem, 4 NegfLead, 5 NegfLsItem, 6 NegfLsProblem) so bindings
+ * can verify their mirrors; 0 if unknown. */
 size_t negf_abi_struct_size(int which);
 
 #ifdef __cplusplus

@@ -43,6 +43,9 @@ def test_struct_mirrors_match_c_sizes():
     assert lib.negf_abi_struct_size(1) == _lib.DEVICE_DTYPE.itemsize
     assert lib.negf_abi_struct_size(2) == _lib.ITEM_DTYPE.itemsize
     assert lib.negf_abi_struct_size(3) == ctypes.sizeof(_lib.NegfRgfProblem)
+    assert lib.negf_abi_struct_size(4) == _lib.LEAD_DTYPE.itemsize
+    assert lib.negf_abi_struct_size(5) == _lib.LS_ITEM_DTYPE.itemsize
+    assert lib.negf_abi_struct_size(6) == ctypes.sizeof(_lib.NegfLsProblem)
 
 
 def test_scratch_query_without_gpu():

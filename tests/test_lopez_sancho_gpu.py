@@ -1,0 +1,98 @@
+"""Lopez-Sancho decimation on the GPU against the reference fixtures, the
+oracle and the analytic 1-D chain; failure statuses map to the reference's
+exceptions.  FP64 tolerance: 1e-9 relative (max-norm) on g_s and Sigma -- the
+decimation is an iterated fixed point whose last digits depend on the
+(LAPACK vs Gauss-Jordan) solve order."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import lead_oracle
+from tests.goldens import Golden
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-9
+
+
+def _rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.mark.parametrize("lead", ["chain", "rand_left", "rand_right"])
+def test_self_energy_matches_reference_fixture(lead):
+    from dpnegf_b200.surface_green import selfEnergy
+    g = Golden("lopez_sancho")
+    p = lead + "/"
+    Eref = float(g[p + "E_ref"]) if g.has(p + "E_ref") else 0.0
+    for i, e in enumerate(g[p + "energy"]):
+        sig, gs = selfEnergy(hL=g[p + "hL"], hLL=g[p + "hLL"], sL=g[p + "sL"], sLL=g[p + "sLL"], ee=float(e),
+                             hDL=g[p + "hDL"], sDL=g[p + "sDL"], etaLead=float(g[p + "eta"]), E_ref=Eref)
+        assert sig.dtype == torch.complex128 and sig.device.type == "cpu"
+        assert _rel(gs.numpy(), g[p + "gs"][i]) < RTOL, (lead, e)
+        assert _rel(sig.numpy(), g[p + "sigma"][i]) < RTOL, (lead, e)
+
+
+def test_surface_green_numpy_contract():
+    from dpnegf_b200.surface_green import surface_green
+    g = Golden("lopez_sancho")
+    gs = surface_green(g["chain/hL"], g["chain/hLL"], g["chain/sL"], g["chain/sLL"], 0.7 + 1e-6j)
+    assert isinstance(gs, np.ndarray) and gs.dtype == np.complex128
+    assert _rel(gs, g["chain/gs"][3]) < RTOL
+
+
+@pytest.mark.parametrize("n", [40, 150, 200])
+def test_batched_decimation_matches_oracle(n):
+    """Many (lead, energy) items in one launch; n > 128 exercises the two-level inverse."""
+    from dpnegf_b200 import workload
+    from dpnegf_b200.surface_green import LeadArena, LeadBlocks, self_energies
+    dev = workload.random_device(n, 3, seed=n)
+    leads = [LeadBlocks(l.hL, l.hLL, l.sL, l.sLL, l.hDL, l.sDL) for l in (dev.lead_L, dev.lead_R)]
+    arena = LeadArena(leads)
+    E = np.array([-1.1, 0.2, 0.9])
+    idx = [0, 1, 0, 1, 0, 1]
+    Es = np.repeat(E, 2)
+    res = self_energies(arena, idx, Es, 1e-4, E_ref=0.01, want_gs=True)
+    # 0 = converged, 1 = converged with the reference's "not-so-well converged" warning
+    assert np.all((res.status == 0) | (res.status == 1)), res.status
+    for k, (li, e) in enumerate(zip(idx, Es)):
+        L = (dev.lead_L, dev.lead_R)[li]
+        sig, gs, st, it = lead_oracle.self_energy(L.hL.numpy(), L.hLL.numpy(), L.sL.numpy(), L.sLL.numpy(), e,
+                                                  L.hDL.numpy(), L.sDL.numpy(), etaLead=1e-4, E_ref=0.01)
+        assert st in (lead_oracle.LS_OK, lead_oracle.LS_WARN)
+        assert abs(int(res.iters[k]) - it) <= 1
+        assert _rel(res.gs[k].cpu().numpy(), gs) < RTOL
+        assert _rel(res.sigma[k].cpu().numpy(), sig) < RTOL
+
+
+def test_chain_surface_green_is_analytic():
+    from dpnegf_b200 import workload
+    from dpnegf_b200.surface_green import LeadArena, LeadBlocks, self_energies
+    c = workload.chain_device(L=2)
+    L = c.lead_R
+    arena = LeadArena([LeadBlocks(L.hL, L.hLL, L.sL, L.sLL, L.hDL, L.sDL)])
+    E = np.linspace(-2.8, 2.8, 29)
+    res = self_energies(arena, [0] * len(E), E, 1e-6)
+    for k, e in enumerate(E):
+        z = e + 1e-6j
+        root = np.sqrt(z * z - 4.0 + 0j)
+        g1 = (z - root) / 2.0
+        if g1.imag > 0:
+            g1 = (z + root) / 2.0
+        assert abs(res.sigma[k][1, 1].item() - g1) < 1e-6
+
+
+def test_non_convergent_lead_reports_status():
+    """eta = 0 inside the band: |alpha|+|beta| never decays; the kernel stops after
+    101 steps with a status, the host raises like the reference."""
+    from dpnegf_b200 import workload
+    from dpnegf_b200 import _lib
+    from dpnegf_b200.surface_green import LeadArena, LeadBlocks, self_energies
+    c = workload.chain_device(L=2)
+    L = c.lead_R
+    arena = LeadArena([LeadBlocks(L.hL, L.hLL, L.sL, L.sLL, L.hDL, L.sDL)])
+    res = self_energies(arena, [0], [0.3], 0.0, check=False)
+    assert res.status[0] in (_lib.NEGF_ERR_LS_NOT_CONVERGED, _lib.NEGF_ERR_SINGULAR, _lib.NEGF_ERR_LS_RESIDUAL)
+    assert res.iters[0] <= 101
+    with pytest.raises((RuntimeError, ArithmeticError)):
+        self_energies(arena, [0], [0.3], 0.0)

@@ -4,8 +4,8 @@
 //
 // One CTA of 256 threads (8 warps) walks the 64x64 output tiles of C; each
 // tile streams 16-wide k-slabs of op(A) and op(B) into padded shared-memory
-// tiles with cp.async (double buffered).  Each warp owns a 32x16 sub-tile and
-// forms every complex product with three real DMMAs (Gauss/3M):
+// tiles with cp.async (3-stage ring).  Each warp owns a 32x16 sub-tile and
+// forms every complex product with three real DMMA m16n8k8 (Gauss/3M):
 //   T1 = Ar*Br, T2 = Ai*Bi, T3 = (Ar+Ai)*(Br+Bi);  Re = T1-T2, Im = T3-T1-T2.
 // Shared-memory pitches are chosen so the DMMA fragment reads (one 16-byte
 // complex per lane) are bank-conflict free for every operand orientation.
@@ -99,48 +99,60 @@ NEGF_DEV void load_b_tile(cplx* sB, const GemmArgs& g, int k0, int n0, int tid) 
 }
 
 struct Acc3M {
-  double t1[4][2][2], t2[4][2][2], t3[4][2][2];
+  double t1[2][2][4], t2[2][2][4], t3[2][2][4];  // [m16 frag][n8 frag][c0..c3]
   NEGF_DEV void zero() {
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
       for (int j = 0; j < 2; ++j)
 #pragma unroll
-        for (int e = 0; e < 2; ++e) t1[i][j][e] = t2[i][j][e] = t3[i][j][e] = 0.0;
+        for (int e = 0; e < 4; ++e) t1[i][j][e] = t2[i][j][e] = t3[i][j][e] = 0.0;
   }
 };
 
-// One warp: ksteps x (k=4) slabs of its 32x16 sub-tile.  Fragment reads go
-// through the index functors so the same loop serves the GEMM tiles and the
-// Gauss-Jordan panel update.
+// Position in the warp's 32x16 sub-tile of accumulator element (i, j, e).
+NEGF_DEV int acc_row(int i, int e, int wm, int lane) { return wm + 16 * i + (lane >> 2) + ((e & 2) ? 8 : 0); }
+NEGF_DEV int acc_col(int j, int e, int wn, int lane) { return wn + 8 * j + 2 * (lane & 3) + (e & 1); }
+
+// One warp: ksteps x (k=8) slabs of its 32x16 sub-tile (2 x 2 DMMA m16n8k8
+// fragments per real plane).  Fragment reads go through the index functors
+// so the same loop serves the GEMM tiles and the Gauss-Jordan panel update.
 template <bool CONJ_A, bool CONJ_B, class AIdx, class BIdx>
 NEGF_DEV void warp_mma_3m(Acc3M& acc, const cplx* sA, const cplx* sB, int ksteps, int wm, int wn, int lane,
                           AIdx aidx, BIdx bidx) {
   const int gr = lane >> 2, gc = lane & 3;
   for (int ks = 0; ks < ksteps; ++ks) {
-    const int kk = ks * 4 + gc;
-    double ar[4], ai[4], as[4], br[2], bi[2], bs[2];
+    const int k0 = ks * 8 + gc;
+    double ar[2][4], ai[2][4], as[2][4], br[2][2], bi[2][2], bs[2][2];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      cplx a = sA[aidx(wm + i * 8 + gr, kk)];
-      ar[i] = a.x;
-      ai[i] = CONJ_A ? -a.y : a.y;
-      as[i] = ar[i] + ai[i];
+    for (int i = 0; i < 2; ++i) {
+      const int r = wm + 16 * i + gr;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        cplx a = sA[aidx(r + ((e & 1) ? 8 : 0), k0 + ((e & 2) ? 4 : 0))];
+        ar[i][e] = a.x;
+        ai[i][e] = CONJ_A ? -a.y : a.y;
+        as[i][e] = ar[i][e] + ai[i][e];
+      }
     }
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
-      cplx b = sB[bidx(kk, wn + j * 8 + gr)];
-      br[j] = b.x;
-      bi[j] = CONJ_B ? -b.y : b.y;
-      bs[j] = br[j] + bi[j];
+      const int c = wn + 8 * j + gr;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        cplx b = sB[bidx(k0 + 4 * e, c)];
+        br[j][e] = b.x;
+        bi[j][e] = CONJ_B ? -b.y : b.y;
+        bs[j][e] = br[j][e] + bi[j][e];
+      }
     }
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
-        dmma884(acc.t1[i][j][0], acc.t1[i][j][1], ar[i], br[j]);
-        dmma884(acc.t2[i][j][0], acc.t2[i][j][1], ai[i], bi[j]);
-        dmma884(acc.t3[i][j][0], acc.t3[i][j][1], as[i], bs[j]);
+        dmma1688(acc.t1[i][j], ar[i], br[j]);
+        dmma1688(acc.t2[i][j], ai[i], bi[j]);
+        dmma1688(acc.t3[i][j], as[i], bs[j]);
       }
   }
 }
@@ -148,15 +160,14 @@ NEGF_DEV void warp_mma_3m(Acc3M& acc, const cplx* sA, const cplx* sB, int ksteps
 // Visit every accumulator element of this warp: f(row, col, value).
 template <class F>
 NEGF_DEV void acc_foreach(const Acc3M& acc, int wm, int wn, int lane, F f) {
-  const int gr = lane >> 2, gc = lane & 3;
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
     for (int j = 0; j < 2; ++j)
 #pragma unroll
-      for (int e = 0; e < 2; ++e) {
+      for (int e = 0; e < 4; ++e) {
         double t1 = acc.t1[i][j][e], t2 = acc.t2[i][j][e], t3 = acc.t3[i][j][e];
-        f(wm + i * 8 + gr, wn + j * 8 + 2 * gc + e, cmk(t1 - t2, t3 - t1 - t2));
+        f(acc_row(i, e, wm, lane), acc_col(j, e, wn, lane), cmk(t1 - t2, t3 - t1 - t2));
       }
 }
 
@@ -213,7 +224,7 @@ __device__ __noinline__ void cta_gemm_epi(const GemmArgs g, cplx* smem, const Ep
           load_b_tile<OPB>(sB(nx % GT_STAGES), g, nx * GT_K, n0, tid);
         }
         cp_async_commit();
-        warp_mma_3m<CA, CB>(acc, sA(kt % GT_STAGES), sB(kt % GT_STAGES), GT_K / 4, wm, wn, lane, AI(), BI());
+        warp_mma_3m<CA, CB>(acc, sA(kt % GT_STAGES), sB(kt % GT_STAGES), GT_K / 8, wm, wn, lane, AI(), BI());
       }
       acc_foreach(acc, wm, wn, lane, [&](int r, int c, cplx v) {
         int m = m0 + r, n = n0 + c;

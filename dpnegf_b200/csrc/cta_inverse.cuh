@@ -115,7 +115,6 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
   double* red_v = reinterpret_cast<double*>(s_misc + 48);  // [2][NWARP]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = (warp >> 2) * 32, wn = (warp & 3) * 16;
-  const int gr = lane >> 2, gc = lane & 3;
   // Panel rows owned by this thread: tid + 256 r, r < RT (n <= 256 RT).
   // Bit r of `used` is set once that row has served as a pivot.
   unsigned used = 0u;
@@ -237,12 +236,12 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
       pc->mark(PH_INV_PANEL);
 
       // ---- apply the panel to the block's other columns, one 64-wide tile at a time
-      auto load_r = [&](cplx* R, int c0) {
+      auto load_r = [&](cplx* Rt, int c0) {
         for (int e = tid; e < NB * GT_N; e += CTA_THREADS) {
           int kk = e / GT_N, cc = e % GT_N;
           bool v = (kk < w && c0 + cc < c_hi);
           const cplx* src = v ? W + (int64_t)piv[p0 + kk] * ldw + c0 + cc : W;
-          cp_async16(R + kk * RP + cc, src, v);
+          cp_async16(Rt + kk * RP + cc, src, v);
         }
         cp_async_commit();
       };
@@ -255,34 +254,34 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
       if (ntile > 0) load_r(Rb[0], tiles[0]);
       for (int t = 0; t < ntile; ++t) {
         const int c0 = tiles[t];
-        cplx* R = Rb[t & 1];
+        cplx* Rt = Rb[t & 1];
         if (t + 1 < ntile) load_r(Rb[(t + 1) & 1], tiles[t + 1]);
         else cp_async_commit();
         cp_async_wait<1>();
         __syncthreads();
         for (int r0 = 0; r0 < n; r0 += GT_M) {
           // fetch this warp's slice of W (the addend) ahead of the tensor-core work
-          cplx old[4][2][2];
+          cplx old[2][2][4];
 #pragma unroll
-          for (int i = 0; i < 4; ++i)
+          for (int i = 0; i < 2; ++i)
 #pragma unroll
             for (int j = 0; j < 2; ++j)
 #pragma unroll
-              for (int e = 0; e < 2; ++e) {
-                int row = r0 + wm + i * 8 + gr, col = c0 + wn + j * 8 + 2 * gc + e;
+              for (int e = 0; e < 4; ++e) {
+                int row = r0 + acc_row(i, e, wm, lane), col = c0 + acc_col(j, e, wn, lane);
                 old[i][j][e] = cmk(0.0, 0.0);
                 if (row < n && col < c_hi) old[i][j][e] = ldg_early(W + (int64_t)row * ldw + col);
               }
           Acc3M acc;
           acc.zero();
-          warp_mma_3m<false, false>(acc, P + (size_t)r0 * PP, R, NB / 4, wm, wn, lane, PanelIdx{PP}, RIdx());
+          warp_mma_3m<false, false>(acc, P + (size_t)r0 * PP, Rt, NB / 8, wm, wn, lane, PanelIdx{PP}, RIdx());
 #pragma unroll
-          for (int i = 0; i < 4; ++i)
+          for (int i = 0; i < 2; ++i)
 #pragma unroll
             for (int j = 0; j < 2; ++j)
 #pragma unroll
-              for (int e = 0; e < 2; ++e) {
-                int row = r0 + wm + i * 8 + gr, col = c0 + wn + j * 8 + 2 * gc + e;
+              for (int e = 0; e < 4; ++e) {
+                int row = r0 + acc_row(i, e, wm, lane), col = c0 + acc_col(j, e, wn, lane);
                 if (row < n && col < c_hi && (col < p0 || col >= p0 + w)) {
                   double t1 = acc.t1[i][j][e], t2 = acc.t2[i][j][e], t3 = acc.t3[i][j][e];
                   cplx v = cmk(t1 - t2, t3 - t1 - t2);

@@ -65,6 +65,17 @@ NEGF_DEV void dmma884(double& c0, double& c1, double a, double b) {
                : "d"(a), "d"(b));
 }
 
+// FP64 tensor-core MMA, D(16x8) += A(16x8, row) * B(8x8, col).
+// Fragment ownership for lane l (g = l/4, t = l%4):
+//   A: a0 (g, t), a1 (g+8, t), a2 (g, t+4), a3 (g+8, t+4)
+//   B: b0 (t, g), b1 (t+4, g)
+//   C: c0 (g, 2t), c1 (g, 2t+1), c2 (g+8, 2t), c3 (g+8, 2t+1)
+NEGF_DEV void dmma1688(double* c, const double* a, const double* b) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+               : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+               : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
 // Operand transforms for the tile GEMM.
 enum Op : int { OP_N = 0, OP_C = 1 /* conjugate transpose */, OP_K = 2 /* conjugate */ };
 

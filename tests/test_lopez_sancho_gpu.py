@@ -61,8 +61,11 @@ def test_batched_decimation_matches_oracle(n):
                                                   L.hDL.numpy(), L.sDL.numpy(), etaLead=1e-4, E_ref=0.01)
         assert st in (lead_oracle.LS_OK, lead_oracle.LS_WARN)
         assert abs(int(res.iters[k]) - it) <= 1
-        assert _rel(res.gs[k].cpu().numpy(), gs) < RTOL
-        assert _rel(res.sigma[k].cpu().numpy(), sig) < RTOL
+        # an item the reference only "not-so-well" converges (residual in (1e-8, 3e-5))
+        # is fixed only to about that residual: compare it at 1e-7
+        tol = RTOL if res.status[k] == 0 else 1e-7
+        assert _rel(res.gs[k].cpu().numpy(), gs) < tol
+        assert _rel(res.sigma[k].cpu().numpy(), sig) < tol
 
 
 def test_chain_surface_green_is_analytic():

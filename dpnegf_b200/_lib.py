@@ -35,6 +35,8 @@ TRANS = 1 << 6
 ORB_DOS = 1 << 7
 LESSER = 1 << 8
 DOS = 1 << 9
+ORB_GDIAG = 1 << 10
+ORB_AR = 1 << 11
 PHASES = ("form", "gemm_fwd", "inv_stage", "inv_panel", "inv_update", "inv_gather", "gemm_bwd", "lesser",
           "dos", "trans", "other")
 
@@ -87,6 +89,8 @@ class NegfRgfProblem(ctypes.Structure):
         ("trans", ctypes.c_void_p),
         ("orb_dos", ctypes.c_void_p),
         ("dos", ctypes.c_void_p),
+        ("orb_g", ctypes.c_void_p),
+        ("orb_ar", ctypes.c_void_p),
         ("status", ctypes.c_void_p),
         ("flags", ctypes.c_uint32),
         ("n_slots", ctypes.c_int32),

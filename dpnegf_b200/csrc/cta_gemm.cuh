@@ -117,7 +117,11 @@ NEGF_DEV int acc_col(int j, int e, int wn, int lane) { return wn + 8 * j + 2 * (
 // One warp: ksteps x (k=8) slabs of its 32x16 sub-tile (2 x 2 DMMA m16n8k8
 // fragments per real plane).  Fragment reads go through the index functors
 // so the same loop serves the GEMM tiles and the Gauss-Jordan panel update.
-template <bool CONJ_A, bool CONJ_B, class AIdx, class BIdx>
+// G3 selects the complex product: Gauss/3M (three real MMAs, t1..t3) or the
+// conventional 4M form (four real MMAs into t1 = Re, t2 = Im), whose
+// componentwise error bound is tighter -- used where an iteration amplifies
+// rounding (the lead decimation).
+template <bool CONJ_A, bool CONJ_B, bool G3 = true, class AIdx, class BIdx>
 NEGF_DEV void warp_mma_3m(Acc3M& acc, const cplx* sA, const cplx* sB, int ksteps, int wm, int wn, int lane,
                           AIdx aidx, BIdx bidx) {
   const int gr = lane >> 2, gc = lane & 3;
@@ -146,29 +150,51 @@ NEGF_DEV void warp_mma_3m(Acc3M& acc, const cplx* sA, const cplx* sB, int ksteps
         bs[j][e] = br[j][e] + bi[j][e];
       }
     }
+    if (G3) {
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+      for (int i = 0; i < 2; ++i)
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        dmma1688(acc.t1[i][j], ar[i], br[j]);
-        dmma1688(acc.t2[i][j], ai[i], bi[j]);
-        dmma1688(acc.t3[i][j], as[i], bs[j]);
-      }
+        for (int j = 0; j < 2; ++j) {
+          dmma1688(acc.t1[i][j], ar[i], br[j]);
+          dmma1688(acc.t2[i][j], ai[i], bi[j]);
+          dmma1688(acc.t3[i][j], as[i], bs[j]);
+        }
+    } else {
+      double an[2][4];
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) an[i][e] = -ai[i][e];
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          dmma1688(acc.t1[i][j], ar[i], br[j]);
+          dmma1688(acc.t1[i][j], an[i], bi[j]);
+          dmma1688(acc.t2[i][j], ar[i], bi[j]);
+          dmma1688(acc.t2[i][j], ai[i], br[j]);
+        }
+    }
   }
 }
 
+// Complex value of accumulator element (i, j, e).
+template <bool G3>
+NEGF_DEV cplx acc_value(const Acc3M& acc, int i, int j, int e) {
+  const double t1 = acc.t1[i][j][e], t2 = acc.t2[i][j][e];
+  if (G3) return cmk(t1 - t2, acc.t3[i][j][e] - t1 - t2);
+  return cmk(t1, t2);
+}
+
 // Visit every accumulator element of this warp: f(row, col, value).
-template <class F>
+template <bool G3, class F>
 NEGF_DEV void acc_foreach(const Acc3M& acc, int wm, int wn, int lane, F f) {
 #pragma unroll
   for (int i = 0; i < 2; ++i)
 #pragma unroll
     for (int j = 0; j < 2; ++j)
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        double t1 = acc.t1[i][j][e], t2 = acc.t2[i][j][e], t3 = acc.t3[i][j][e];
-        f(acc_row(i, e, wm, lane), acc_col(j, e, wn, lane), cmk(t1 - t2, t3 - t1 - t2));
-      }
+      for (int e = 0; e < 4; ++e) f(acc_row(i, e, wm, lane), acc_col(j, e, wn, lane), acc_value<G3>(acc, i, j, e));
 }
 
 struct AIdxOp0 { NEGF_DEV int operator()(int m, int k) const { return a_idx<OP_N>(m, k); } };
@@ -191,7 +217,7 @@ struct EpiStore {
 // B.  Ends with __syncthreads(), so whatever epi wrote to global memory is
 // visible to every thread of the CTA on return.  k-slabs flow through a
 // GT_STAGES-deep cp.async ring (one barrier per slab).
-template <int OPA, int OPB, class Epi>
+template <int OPA, int OPB, bool G3, class Epi>
 __device__ __noinline__ void cta_gemm_epi(const GemmArgs g, cplx* smem, const Epi epi) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = (warp >> 2) * 32, wn = (warp & 3) * 16;
@@ -224,9 +250,9 @@ __device__ __noinline__ void cta_gemm_epi(const GemmArgs g, cplx* smem, const Ep
           load_b_tile<OPB>(sB(nx % GT_STAGES), g, nx * GT_K, n0, tid);
         }
         cp_async_commit();
-        warp_mma_3m<CA, CB>(acc, sA(kt % GT_STAGES), sB(kt % GT_STAGES), GT_K / 8, wm, wn, lane, AI(), BI());
+        warp_mma_3m<CA, CB, G3>(acc, sA(kt % GT_STAGES), sB(kt % GT_STAGES), GT_K / 8, wm, wn, lane, AI(), BI());
       }
-      acc_foreach(acc, wm, wn, lane, [&](int r, int c, cplx v) {
+      acc_foreach<G3>(acc, wm, wn, lane, [&](int r, int c, cplx v) {
         int m = m0 + r, n = n0 + c;
         if (m < g.M && n < g.N) epi(m, n, v);
       });
@@ -237,9 +263,9 @@ __device__ __noinline__ void cta_gemm_epi(const GemmArgs g, cplx* smem, const Ep
 }
 
 // C = alpha op(A) op(B) + beta D (D may alias C; C must not alias A or B).
-template <int OPA, int OPB>
+template <int OPA, int OPB, bool G3 = true>
 NEGF_DEV void cta_gemm(const GemmArgs& g, cplx* smem) {
-  cta_gemm_epi<OPA, OPB>(g, smem, EpiStore{g});
+  cta_gemm_epi<OPA, OPB, G3>(g, smem, EpiStore{g});
 }
 
 }  // namespace negf

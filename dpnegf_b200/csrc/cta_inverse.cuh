@@ -97,7 +97,7 @@ struct EpiGJ {
 // Returns 0 on success, 1 if a zero or non-finite pivot was met.  Uniform
 // across the CTA; ends with __syncthreads().  `snap` is global scratch of
 // inv_snapshot_elems(n) complex elements (unused when n <= INV_OB).
-template <int NB, int RT>
+template <int NB, int RT, bool G3>
 __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G, int64_t ldg, char* smem_raw,
                                            PhaseClock* pc, cplx* snap) {
   constexpr int PP = InvLayout<NB>::PP;
@@ -274,7 +274,7 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
               }
           Acc3M acc;
           acc.zero();
-          warp_mma_3m<false, false>(acc, P + (size_t)r0 * PP, Rt, NB / 8, wm, wn, lane, PanelIdx{PP}, RIdx());
+          warp_mma_3m<false, false, G3>(acc, P + (size_t)r0 * PP, Rt, NB / 8, wm, wn, lane, PanelIdx{PP}, RIdx());
 #pragma unroll
           for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -283,8 +283,7 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
               for (int e = 0; e < 4; ++e) {
                 int row = r0 + acc_row(i, e, wm, lane), col = c0 + acc_col(j, e, wn, lane);
                 if (row < n && col < c_hi && (col < p0 || col >= p0 + w)) {
-                  double t1 = acc.t1[i][j][e], t2 = acc.t2[i][j][e], t3 = acc.t3[i][j][e];
-                  cplx v = cmk(t1 - t2, t3 - t1 - t2);
+                  cplx v = acc_value<G3>(acc, i, j, e);
                   int lc = pinv[row];
                   bool is_piv = (lc >= p0 && lc < p0 + w);
                   W[(int64_t)row * ldw + col] = is_piv ? v : cadd(old[i][j][e], v);
@@ -314,11 +313,11 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
       __syncthreads();
       if (c_lo > 0) {
         GemmArgs g = gemm_args(n, c_lo, kb, W + c_lo, ldw, snap, n, W, ldw);
-        cta_gemm_epi<OP_N, OP_N>(g, reinterpret_cast<cplx*>(smem_raw), EpiGJ{W, ldw, pinv, c_lo, c_hi, 0});
+        cta_gemm_epi<OP_N, OP_N, G3>(g, reinterpret_cast<cplx*>(smem_raw), EpiGJ{W, ldw, pinv, c_lo, c_hi, 0});
       }
       if (c_hi < n) {
         GemmArgs g = gemm_args(n, n - c_hi, kb, W + c_lo, ldw, snap + c_hi, n, W + c_hi, ldw);
-        cta_gemm_epi<OP_N, OP_N>(g, reinterpret_cast<cplx*>(smem_raw), EpiGJ{W, ldw, pinv, c_lo, c_hi, c_hi});
+        cta_gemm_epi<OP_N, OP_N, G3>(g, reinterpret_cast<cplx*>(smem_raw), EpiGJ{W, ldw, pinv, c_lo, c_hi, c_hi});
       }
       pc->mark(PH_INV_UPDATE);
     }
@@ -336,10 +335,12 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
   return flag;
 }
 
+// G3: complex products of the rank updates (Gauss/3M or conventional 4M).
+template <bool G3 = true>
 NEGF_DEV int cta_inverse(cplx* W, int64_t ldw, int n, cplx* G, int64_t ldg, char* smem_raw, PhaseClock* pc,
                          cplx* snap) {
-  if (n <= 256) return cta_inverse_nb<32, 1>(W, ldw, n, G, ldg, smem_raw, pc, snap);
-  return cta_inverse_nb<16, 2>(W, ldw, n, G, ldg, smem_raw, pc, snap);
+  if (n <= 256) return cta_inverse_nb<32, 1, G3>(W, ldw, n, G, ldg, smem_raw, pc, snap);
+  return cta_inverse_nb<16, 2, G3>(W, ldw, n, G, ldg, smem_raw, pc, snap);
 }
 
 }  // namespace negf

@@ -15,6 +15,9 @@
 //   g_s = (zS - eps_s)^-1, accepted when
 //     max |(zS - H - (z s01 - h01) g_s (z s10 - h10)) g_s - I| < 3e-5
 //     (warning status above 1e-8)
+// Complex products use the conventional 4M form: the doubling iteration
+// amplifies the looser componentwise error of Gauss/3M products to ~1e-9 on
+// g_s at ill-conditioned energies.
 // and the self-energy product of selfEnergy (:73-86):
 //   Sigma = (E S_DL - H_DL) g_s[:b,:b] (E S_DL^H - H_DL^H),   E without i*eta,
 // or the bulk form Sigma = (E S - H) - g_s^-1 when the lead has no H_DL.
@@ -76,7 +79,7 @@ NEGF_DEV void gemm_ls(cplx* smem, int M, int N, int K, const cplx* A, int64_t ld
   GemmArgs g = gemm_args(M, N, K, A, lda, B, ldb, C, ldc);
   g.alpha = alpha;
   if (D) { g.D = D; g.ldd = ldd; g.beta = beta; g.use_d = true; }
-  cta_gemm<OPA, OPB>(g, smem);
+  cta_gemm<OPA, OPB, false>(g, smem);  // conventional 4M products: see warp_mma_3m
 }
 
 NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, char* smem_raw, double* red) {
@@ -115,7 +118,7 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
     it_n = iter;
     // A = zS - eps
     cta_shift_form(A, eps, S, z, cmk(-1.0, 0.0), (int)n2, smem);
-    bad |= cta_inverse(A, n, n, Ainv, n, smem_raw, &pc, snap);
+    bad |= cta_inverse<false>(A, n, n, Ainv, n, smem_raw, &pc, snap);
     gemm_ls<OP_N, OP_N>(smem, n, n, n, Ainv, n, alpha, n, Xa, n);
     gemm_ls<OP_N, OP_N>(smem, n, n, n, Ainv, n, beta, n, Xb, n);
     gemm_ls<OP_N, OP_N>(smem, n, n, n, beta, n, Xa, n, T, n);  // beta Xa
@@ -151,7 +154,7 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
     cplx* gs = it.gs ? reinterpret_cast<cplx*>(it.gs) : gsb;
     // g_s = (zS - eps_s)^-1
     cta_shift_form(A, epss, S, z, cmk(-1.0, 0.0), (int)n2, smem);
-    bad |= cta_inverse(A, n, n, gs, n, smem_raw, &pc, snap);
+    bad |= cta_inverse<false>(A, n, n, gs, n, smem_raw, &pc, snap);
     // residual: (zS - H - (z s01 - h01) g_s (z s10 - h10)) g_s - I
     // z s01 - h01
 #pragma unroll 4
@@ -193,7 +196,7 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
       } else {
         // bulk form: Sigma = (E S - H) - g_s^-1
         cta_shift_form(A, gs, nullptr, cmk(0.0, 0.0), ONE, (int)n2, smem);
-        bad |= cta_inverse(A, n, n, Xa, n, smem_raw, &pc, snap);
+        bad |= cta_inverse<false>(A, n, n, Xa, n, smem_raw, &pc, snap);
 #pragma unroll 4
         for (int e = threadIdx.x; e < n2; e += CTA_THREADS) sig[e] = csub(csub(cmul(E, S[e]), H[e]), Xa[e]);
         __syncthreads();

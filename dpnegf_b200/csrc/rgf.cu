@@ -218,7 +218,29 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
 
   // ----------------------------------------------------------- backward sweep
   const int nN = blk[K - 1].n;
-  const bool need_gt = (fl & (NEGF_OUT_GTRANS | NEGF_OUT_GR_LC | NEGF_TRANS)) != 0;
+  const bool need_gt = (fl & (NEGF_OUT_GTRANS | NEGF_OUT_GR_LC | NEGF_TRANS | NEGF_ORB_AR)) != 0;
+  cplx* orbg = (fl & NEGF_ORB_GDIAG) ? reinterpret_cast<cplx*>(P.orb_g) + it.orb : nullptr;
+  double* orbar = ((fl & NEGF_ORB_AR) && seR) ? P.orb_ar + it.orb : nullptr;
+  const int crA = seR ? min(nN, it.nse_r) : 0;
+  // diag(G_qN Gamma_R G_qN^H) of block q from gt = G_qN (nq x nN); Gamma_R corner in sb.Nu
+  auto spectral_diag = [&](double* dst, const cplx* gtq, int nq) {
+    gemm<OP_N, OP_N>(smem, nq, crA, crA, gtq + (nN - crA), nN, sb.Nu, crA, sb.W, crA);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = warp; i < nq; i += CTA_THREADS / 32) {
+      double acc = 0.0;
+      for (int l = lane; l < crA; l += 32) {
+        cplx y = sb.W[(int64_t)i * crA + l], g = gtq[(int64_t)i * nN + (nN - crA) + l];
+        acc += y.x * g.x + y.y * g.y;  // Re(y conj(g))
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+      if (lane == 0) dst[i] = acc;
+    }
+    __syncthreads();
+  };
+  auto gdiag = [&](cplx* dst, const cplx* G, int nq) {
+    for (int i = threadIdx.x; i < nq; i += CTA_THREADS) dst[i] = G[(int64_t)i * nq + i];
+  };
   const bool want_dos = (fl & (NEGF_ORB_DOS | NEGF_DOS)) != 0;
   double* orb = (fl & NEGF_ORB_DOS) ? P.orb_dos + it.orb : nullptr;
   double dsum = 0.0;  // per-thread partial of sum_i -Im diag(GS)_i / pi
@@ -251,6 +273,12 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
     __syncthreads();
     pc.mark(PH_DOS);
   }
+  if (orbg) gdiag(orbg + blk[K - 1].orb0, gptr(K - 1), nN);
+  if (orbar) {
+    form_gamma(sb.Nu, seR, it.nse_r, it.nse_r - crA, crA);
+    __syncthreads();
+    spectral_diag(orbar + blk[K - 1].orb0, gt, nN);
+  }
   int tog = 0;
   for (int q = K - 2; q >= 0; --q) {
     const NegfBlock& b = blk[q];
@@ -276,6 +304,8 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
       tog ^= 1;
     }
     pc.mark(PH_GEMM_BWD);
+    if (orbg) gdiag(orbg + b.orb0, grd, nq);
+    if (orbar) spectral_diag(orbar + b.orb0, gt, nq);
     if (lesser) {
       const cplx* gin = ginptr(q);
       cplx* gnl = b.o_gnl >= 0 ? out + b.o_gnl + row * szu : sb.Nl;
@@ -407,6 +437,8 @@ int negf_rgf_run(const NegfRgfProblem* p, void* stream) {
   if ((p->flags & NEGF_TRANS) && !p->trans) return NEGF_ERR_ARGUMENT;
   if ((p->flags & NEGF_ORB_DOS) && !p->orb_dos) return NEGF_ERR_ARGUMENT;
   if ((p->flags & NEGF_DOS) && !p->dos) return NEGF_ERR_ARGUMENT;
+  if ((p->flags & NEGF_ORB_GDIAG) && !p->orb_g) return NEGF_ERR_ARGUMENT;
+  if ((p->flags & NEGF_ORB_AR) && !p->orb_ar) return NEGF_ERR_ARGUMENT;
   const uint32_t blockouts = NEGF_OUT_GTRANS | NEGF_OUT_GR_LC | NEGF_OUT_GRD | NEGF_OUT_GRL | NEGF_OUT_GRU |
                              NEGF_OUT_GR_LEFT | NEGF_LESSER;
   if ((p->flags & blockouts) && !p->out) return NEGF_ERR_ARGUMENT;

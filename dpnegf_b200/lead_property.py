@@ -1,0 +1,172 @@
+"""Lead object with GPU self-energies (mirror of negf/lead_property.py).
+
+Same constructor, attributes and methods as the reference ``LeadProperty``
+(:30-460): ``self_energy`` sets ``self.se``, ``gamma`` is i(Sigma - Sigma^H),
+``fermi_dirac`` uses ``chemiPot_lead = efermi - voltage``.  The self-energy is
+computed by the batched Lopez-Sancho kernel; ``energy`` may also be a 1-D
+tensor of energies, in which case ``self.se`` is ``[B, n, n]`` from a single
+launch (the reference computes one energy per call and stacks them in the
+runner, runner/NEGF.py:762-778).  Saved self-energies are read back in the
+``pth`` format; the HDF5 cache and the joblib pool of the reference are not
+part of this package.
+"""
+import logging
+import os
+from typing import List
+
+import numpy as np
+import torch
+from scipy.constants import Boltzmann
+
+from .bloch import Bloch
+from .surface_green import LeadArena, LeadBlocks, self_energies
+
+log = logging.getLogger(__name__)
+eV2J = 1.6021766208e-19  # J per eV, as in dpnegf/utils/constants.py
+
+
+class LeadProperty(object):
+    def __init__(self, tab, hamiltonian, structure, results_path, voltage,
+                 structure_leads_fold=None, bloch_sorted_indice=None, useBloch: bool = False,
+                 bloch_factor: List[int] = [1, 1, 1], bloch_R_list=None,
+                 e_T=300, efermi: float = 0.0, E_ref: float = None) -> None:
+        self.hamiltonian = hamiltonian
+        self.structure = structure
+        self.tab = tab
+        self.voltage = voltage
+        self.results_path = results_path
+        self.kBT = Boltzmann * e_T / eV2J
+        self.e_T = e_T
+        self.efermi = efermi
+        self.E_ref = efermi if E_ref is None else E_ref
+        self.chemiPot_lead = efermi - voltage
+        self.kpoint = None
+        self.voltage_old = None
+        self.useBloch = useBloch
+        self.bloch_factor = bloch_factor
+        self.bloch_sorted_indice = bloch_sorted_indice
+        self.bloch_R_list = bloch_R_list
+        self.structure_leads_fold = structure_leads_fold
+        self._arena = None
+        self._arena_key = None
+        if self.useBloch:
+            assert self.bloch_sorted_indice is not None
+            assert self.bloch_R_list is not None
+            assert self.bloch_factor is not None
+            assert self.structure_leads_fold is not None
+
+    # ------------------------------------------------------------------ API
+    def self_energy(self, kpoint, energy, eta_lead: float = 1e-5, method: str = "Lopez-Sancho",
+                    save_path: str = None, save_format: str = "pth", se_info_display: bool = False,
+                    HS_inmem: bool = True):
+        """Set ``self.se`` for ``kpoint`` at ``energy`` (scalar or [B], relative to E_ref)."""
+        assert len(np.array(kpoint).reshape(-1)) == 3
+        if not isinstance(energy, torch.Tensor):
+            energy = torch.tensor(energy)
+        if save_path is not None and save_format == "pth" and os.path.isfile(save_path):
+            if se_info_display:
+                log.info(f"Loading {self.tab} self-energy from {save_path}")
+            self.se = torch.load(save_path, weights_only=False)
+            return
+        self.se = self.self_energy_cal(kpoint, energy, eta_lead=eta_lead, method=method, HS_inmem=HS_inmem)
+
+    def self_energy_cal(self, kpoint, energy, eta_lead: float = 1e-5, method: str = "Lopez-Sancho",
+                        se_numba_jit=None, HS_inmem: bool = True):
+        if method not in ("Lopez-Sancho",):
+            log.warning(f"sgf_solver {method} is not provided; using Lopez-Sancho")
+        E = torch.as_tensor(energy).to(torch.complex128).reshape(-1).cpu().numpy()
+        scalar = torch.as_tensor(energy).ndim == 0
+        subblocks = self.hamiltonian.get_hs_device(kpoint, only_subblocks=True)
+        if not self.useBloch:
+            key = (tuple(np.asarray(kpoint, dtype=float).reshape(3)), float(self.voltage))
+            if self._arena is None or self._arena_key != key:
+                self.HLk, self.HLLk, self.HDLk, self.SLk, self.SLLk, self.SDLk = \
+                    self.hamiltonian.get_hs_lead(kpoint, tab=self.tab, v=self.voltage)
+                self.voltage_old = self.voltage
+                self.kpoint = torch.tensor(kpoint)
+                hdl, sdl = self.HDL_reduced(torch.as_tensor(self.HDLk), torch.as_tensor(self.SDLk), subblocks)
+                self._arena = LeadArena([LeadBlocks(torch.as_tensor(self.HLk), torch.as_tensor(self.HLLk),
+                                                    torch.as_tensor(self.SLk), torch.as_tensor(self.SLLk),
+                                                    hdl, sdl)])
+                self._arena_key = key
+            res = self_energies(self._arena, [0] * len(E), E, eta_lead, E_ref=self.E_ref)
+            se = torch.stack(res.sigma) if not scalar else res.sigma[0]
+        else:
+            se = self._bloch_self_energy(kpoint, E, eta_lead, subblocks)
+            if scalar:
+                se = se[0]
+        if not HS_inmem:
+            for a in ("HLk", "HLLk", "HDLk", "SLk", "SLLk", "SDLk"):
+                if hasattr(self, a):
+                    delattr(self, a)
+            self._arena = None
+        return se
+
+    def _bloch_self_energy(self, kpoint, E, eta_lead, subblocks):
+        """Bloch-unfolded lead (reference :330-379): decimate every unfolded k on the
+        GPU in one launch, phase-kron and average the surface Green's functions."""
+        self.kpoint = torch.tensor(kpoint)
+        self.voltage_old = self.voltage
+        unfolder = Bloch(self.bloch_factor)
+        kps = unfolder.unfold_points(self.kpoint.tolist())
+        m_size = int(self.bloch_factor[1] * self.bloch_factor[0])
+        leads = []
+        for kb in kps:
+            hL, hLL, hDL, sL, sLL, sDL = self.hamiltonian.get_hs_lead(torch.tensor(kb), tab=self.tab, v=self.voltage)
+            leads.append(LeadBlocks(torch.as_tensor(hL), torch.as_tensor(hLL), torch.as_tensor(sL),
+                                    torch.as_tensor(sLL)))
+            self.HLk, self.HLLk, self.HDLk, self.SLk, self.SLLk, self.SDLk = hL, hLL, hDL, sL, sLL, sDL
+        arena = LeadArena(leads)
+        nk, nE = len(kps), len(E)
+        idx = [ik for ik in range(nk) for _ in range(nE)]
+        res = self_energies(arena, idx, np.tile(E, nk), eta_lead, E_ref=self.E_ref, want_gs=True, want_sigma=False)
+        dev = res.gs[0].device
+        R = [torch.as_tensor(r, dtype=torch.float64) for r in self.bloch_R_list]
+        sgf = None
+        for ik, kb in enumerate(kps):
+            kbt = torch.tensor(kb, dtype=torch.float64)
+            ph = torch.ones(m_size, m_size, dtype=torch.complex128)
+            for i in range(m_size):
+                for j in range(m_size):
+                    if i != j:
+                        ph[i, j] = torch.exp(1j * 2 * torch.pi * torch.dot(R[j] - R[i], kbt))
+            g = torch.stack(res.gs[ik * nE:(ik + 1) * nE])  # [nE, n, n]
+            term = torch.stack([torch.kron(ph.to(dev), g[e]) for e in range(nE)])
+            sgf = term if sgf is None else sgf + term
+        sgf = sgf / nk
+        idxs = torch.as_tensor(self.bloch_sorted_indice, device=dev)
+        sgf = sgf[:, idxs, :][:, :, idxs]
+        hdl, sdl = self.HDL_reduced(torch.as_tensor(self.HDLk), torch.as_tensor(self.SDLk), subblocks)
+        hdl, sdl = hdl.to(dev, torch.complex128), sdl.to(dev, torch.complex128)
+        b = torch.as_tensor(self.HDLk).shape[1]
+        Es = torch.as_tensor(E, device=dev).reshape(-1, 1, 1) + complex(self.E_ref)
+        left = Es * sdl - hdl
+        right = Es * sdl.conj().T - hdl.conj().T
+        return left @ sgf[:, :b, :b] @ right
+
+    @staticmethod
+    def HDL_reduced(HDL: torch.Tensor, SDL: torch.Tensor, subblocks) -> torch.Tensor:
+        """Trim the lead-device coupling to the coupled device rows (reference :386-434)."""
+        assert len(HDL.shape) == 2, "The shape of HDL should be 2."
+        assert len(SDL.shape) == 2, "The shape of SDL should be 2."
+        assert HDL.shape == SDL.shape, "The shape of HDL and SDL should be the same."
+        nz = HDL.nonzero()
+        row_min, row_max = nz.min(dim=0).values[0], nz.max(dim=0).values[0]
+        if HDL.shape[0] == 1:
+            return HDL, SDL
+        if row_min > 0:  # right lead: coupled rows sit at the bottom
+            cut = row_min if subblocks is None else -1 * subblocks[-1]
+            return HDL[cut:, :], SDL[cut:, :]
+        cut = row_max + 1 if subblocks is None else subblocks[0]  # left lead
+        return HDL[:cut, :], SDL[:cut, :]
+
+    def sigmaLR2Gamma(self, se):
+        """Gamma = i (Sigma - Sigma^H)."""
+        return 1j * (se - se.mH)
+
+    def fermi_dirac(self, x) -> torch.Tensor:
+        return 1 / (1 + torch.exp((x - self.chemiPot_lead) / self.kBT))
+
+    @property
+    def gamma(self):
+        return self.sigmaLR2Gamma(self.se)

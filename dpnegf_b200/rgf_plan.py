@@ -137,7 +137,9 @@ class RgfResult:
     dos: Optional[torch.Tensor]      # [n_items] DOS with spin factor 2
     status: torch.Tensor
     blocks: list                     # per device: tag -> list of [B, ...] tensors (tensor for g_trans)
-    phase_cycles: Optional[torch.Tensor] = None  # [n_slots, 8] SM cycles per phase
+    phase_cycles: Optional[torch.Tensor] = None  # [n_slots, NEGF_PHASES] SM cycles per phase
+    orb_g: Optional[torch.Tensor] = None    # concatenated per-item [n_orb] diag(G_qq) (complex)
+    orb_ar: Optional[torch.Tensor] = None   # concatenated per-item [n_orb] diag(G_qN Gamma_R G_qN^H)
 
 
 _FAMILY = {  # output tag -> (flag, block field, shape fn (n_q, n_next, n_last))
@@ -155,7 +157,8 @@ _FAMILY = {  # output tag -> (flag, block field, shape fn (n_q, n_next, n_last))
 
 def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.Tensor]],
         se_r: List[Optional[torch.Tensor]], eta=0.0, E_ref=0.0, outputs=("g_trans", "grd", "grl", "gru"),
-        trans=False, orb_dos=False, dos=False, s_in: Optional[List[List[Optional[torch.Tensor]]]] = None,
+        trans=False, orb_dos=False, dos=False, orb_g=False, orb_ar=False,
+        s_in: Optional[List[List[Optional[torch.Tensor]]]] = None,
         n_slots=None, check=True, stream=None, phase=False, events=None):
     """Run the batched sweep.
 
@@ -189,6 +192,10 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
         flags |= _lib.ORB_DOS
     if dos:
         flags |= _lib.DOS
+    if orb_g:
+        flags |= _lib.ORB_GDIAG
+    if orb_ar:
+        flags |= _lib.ORB_AR
     if lesser:
         flags |= _lib.LESSER
 
@@ -294,6 +301,8 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     trans_t = torch.empty(max(item_cursor, 1), dtype=torch.float64, device=dev) if trans else None
     orb_t = torch.empty(max(orb_cursor, 1), dtype=torch.float64, device=dev) if orb_dos else None
     dos_t = torch.empty(max(item_cursor, 1), dtype=torch.float64, device=dev) if dos else None
+    orbg_t = torch.empty(max(orb_cursor, 1), dtype=C128, device=dev) if orb_g else None
+    orbar_t = torch.zeros(max(orb_cursor, 1), dtype=torch.float64, device=dev) if orb_ar else None
     status_t = torch.empty(max(item_cursor, 1), dtype=torch.int32, device=dev)
     if n_slots is None:
         n_slots = max(1, min(n_items, lib.negf_sm_count()))
@@ -310,6 +319,8 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     prob.trans = trans_t.data_ptr() if trans else None
     prob.orb_dos = orb_t.data_ptr() if orb_dos else None
     prob.dos = dos_t.data_ptr() if dos else None
+    prob.orb_g = orbg_t.data_ptr() if orb_g else None
+    prob.orb_ar = orbar_t.data_ptr() if orb_ar else None
     prob.status = status_t.data_ptr()
     prob.flags = flags
     prob.n_slots = n_slots
@@ -352,4 +363,6 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     return RgfResult(trans=trans_t[:item_cursor] if trans else None,
                      orb_dos=orb_t[:orb_cursor] if orb_dos else None,
                      dos=dos_t[:item_cursor] if dos else None,
-                     status=status_t[:item_cursor], blocks=res_blocks, phase_cycles=phase_t)
+                     status=status_t[:item_cursor], blocks=res_blocks, phase_cycles=phase_t,
+                     orb_g=orbg_t[:orb_cursor] if orb_g else None,
+                     orb_ar=orbar_t[:orb_cursor] if orb_ar else None)

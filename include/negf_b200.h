@@ -54,6 +54,8 @@ extern "C" {
 #define NEGF_ORB_DOS (1u << 7)     /* -Im diag(G S)_i / pi per orbital -> orb_dos[] */
 #define NEGF_LESSER (1u << 8)      /* lesser sweep: gin_left, gnd, gnl, gnu          */
 #define NEGF_DOS (1u << 9)         /* DOS = 2 sum_i (-Im diag(G S)_i / pi) -> dos[]  */
+#define NEGF_ORB_GDIAG (1u << 10)  /* diag(G_qq) per orbital (complex128)  -> orb_g[] */
+#define NEGF_ORB_AR (1u << 11)     /* diag(G_qN Gamma_R G_qN^H) per orbital -> orb_ar[] */
 
 /* Phase indices of NegfRgfProblem.phase_cycles (clock64 cycles per slot). */
 #define NEGF_PHASES 11 /* form, gemm_fwd, inv_stage, inv_panel, inv_update, inv_gather,
@@ -113,6 +115,8 @@ typedef struct NegfRgfProblem {
   double* trans;            /* [n_items] T(E) (NEGF_TRANS) */
   double* orb_dos;          /* per-orbital -Im diag(GS)/pi (NEGF_ORB_DOS) */
   double* dos;              /* [n_items] DOS with spin factor 2 (NEGF_DOS) */
+  double* orb_g;            /* complex128 per-orbital diag(G_qq), item offset = NegfItem.orb (NEGF_ORB_GDIAG) */
+  double* orb_ar;           /* per-orbital diag(G_qN Gamma_R G_qN^H), offset NegfItem.orb (NEGF_ORB_AR) */
   int32_t* status;          /* [n_items] per-item status (always written) */
   uint32_t flags;
   int32_t n_slots;          /* concurrent work slots = CTAs launched */

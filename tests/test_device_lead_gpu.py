@@ -1,0 +1,174 @@
+"""DeviceProperty / LeadProperty / Ozaki mirrors on the GPU against the
+reference fixtures and the oracle (FP64, 1e-10 relative unless stated)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import lead_oracle, rgf_oracle
+from tests.goldens import Golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    a = a.detach().cpu().numpy() if torch.is_tensor(a) else np.asarray(a)
+    b = np.asarray(b)
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+class FakeHamiltonian:
+    """Stands in for NEGFHamiltonianInit: serves fixed BTD blocks and lead blocks."""
+
+    def __init__(self, dev, norbs, leads=None, subblocks=None):
+        self._packed = (dev.hd, dev.sd, dev.hl, dev.su, dev.sl, dev.hu)
+        self.device_norbs = norbs
+        self.leads = leads or {}
+        self.subblocks = subblocks
+
+    def get_hs_device(self, kpoint, V=None, block_tridiagonal=True, only_subblocks=False):
+        if only_subblocks:
+            return self.subblocks
+        return self._packed
+
+    def get_hs_lead(self, kpoint, tab, v):
+        L = self.leads[tab]
+        return (L.hL - v * L.sL, L.hLL - v * L.sLL, L.hDL, L.sL, L.sLL, L.sDL)
+
+
+class FakeLead:
+    def __init__(self, mu, kBT=0.025, voltage=0.0, efermi=0.0):
+        self.se = None
+        self.chemiPot_lead = mu
+        self.kBT = kBT
+        self.voltage = voltage
+        self.efermi = efermi
+
+    def fermi_dirac(self, x):
+        return 1.0 / (1.0 + torch.exp((x - self.chemiPot_lead) / self.kBT))
+
+    @property
+    def gamma(self):
+        return 1j * (self.se - self.se.mH)
+
+
+def _devprop_from_golden(g):
+    from dpnegf_b200 import workload
+    from dpnegf_b200.device_property import DeviceProperty
+    dims = list(g["dims"])
+    dev = workload.BTDDevice(*[[torch.as_tensor(x) for x in g[k]] for k in ("hd", "hu", "hl", "sd", "su", "sl")])
+    dp = DeviceProperty(FakeHamiltonian(dev, list(g["norbs"])), None, "", e_T=300, E_ref=float(g["E_ref"]))
+    dp.kBT = float(g["kBT"])
+    dp.set_leadLR(FakeLead(float(g["muL"])), FakeLead(float(g["muR"])))
+    return dp
+
+
+@pytest.mark.parametrize("case", ["devprop_nonuniform", "devprop_uniform"])
+def test_device_property_matches_reference_fixture(case):
+    g = Golden(case)
+    dp = _devprop_from_golden(g)
+    dp.lead_L.se = torch.as_tensor(g["left_se"])
+    dp.lead_R.se = torch.as_tensor(g["right_se"])
+    dp.cal_green_function(energy=torch.as_tensor(g["energy"]), kpoint=[0.0, 0.0, 0.0],
+                          eta_device=float(g["eta_device"]), block_tridiagonal=True, need_lesser=True)
+    assert _rel(dp.tc, g["out/tc"]) < 1e-10
+    assert _rel(dp.dos, g["out/dos"]) < 1e-10
+    assert _rel(dp.ldos, g["out/ldos"]) < 1e-10
+    for got, want in zip(dp.gnd, g["out/gnd"]):
+        assert _rel(got, want) < 1e-10
+
+
+def test_device_property_scalar_energy_shapes():
+    g = Golden("devprop_uniform")
+    dp = _devprop_from_golden(g)
+    dp.lead_L.se = torch.as_tensor(g["left_se"][1])
+    dp.lead_R.se = torch.as_tensor(g["right_se"][1])
+    dp.cal_green_function(energy=complex(g["energy"][1]), kpoint=[0.0, 0.0, 0.0],
+                          eta_device=float(g["eta_device"]), need_lesser=True)
+    assert dp.tc.ndim == 0 and dp.dos.ndim == 0 and dp.ldos.ndim == 1 and dp.grd[0].ndim == 2
+    assert _rel(dp.tc, g["out/tc"][1]) < 1e-10
+    assert _rel(dp.gnd[0], g["out/gnd"][0][1]) < 1e-10
+
+
+def test_lead_property_self_energy_batch_matches_oracle():
+    from dpnegf_b200 import workload
+    from dpnegf_b200.lead_property import LeadProperty
+    dev = workload.random_device(24, 4, seed=41)
+    ham = FakeHamiltonian(dev, [1] * 96, leads={"lead_L": dev.lead_L, "lead_R": dev.lead_R})
+    for tab in ("lead_L", "lead_R"):
+        lp = LeadProperty(tab, ham, None, "", voltage=0.05, efermi=0.1)
+        E = torch.tensor([-0.8, 0.0, 0.6], dtype=torch.float64)
+        lp.self_energy(kpoint=[0.0, 0.0, 0.0], energy=E, eta_lead=1e-5)
+        assert lp.se.shape == (3, 24, 24)
+        L = (dev.lead_L if tab == "lead_L" else dev.lead_R)
+        hL, hLL, hDL, sL, sLL, sDL = ham.get_hs_lead([0, 0, 0], tab, 0.05)
+        for i, e in enumerate(E.numpy()):
+            sig, _, st, _ = lead_oracle.self_energy(hL.numpy(), hLL.numpy(), sL.numpy(), sLL.numpy(), e,
+                                                    hDL.numpy(), sDL.numpy(), etaLead=1e-5, E_ref=0.1)
+            assert _rel(lp.se[i], sig) < 1e-9
+        lp.self_energy(kpoint=[0.0, 0.0, 0.0], energy=0.6, eta_lead=1e-5)
+        assert lp.se.ndim == 2
+        g = lp.gamma
+        assert torch.allclose(g, g.mH)
+
+
+def test_hdl_reduced_matches_reference_rule():
+    from dpnegf_b200.lead_property import LeadProperty
+    H = torch.zeros(6, 4, dtype=torch.complex128)
+    H[4:, :] = 1.0
+    hr, sr = LeadProperty.HDL_reduced(H, H.clone(), None)
+    assert hr.shape == (2, 4)
+    H2 = torch.zeros(6, 4, dtype=torch.complex128)
+    H2[:3, :] = 1.0
+    hr, _ = LeadProperty.HDL_reduced(H2, H2.clone(), None)
+    assert hr.shape == (3, 4)
+    hr, _ = LeadProperty.HDL_reduced(H2, H2.clone(), [2, 3])
+    assert hr.shape == (2, 4)
+
+
+def _single_block_setup(n=12, seed=3):
+    """One-block device with explicit leads (block_tridiagonal=False style)."""
+    from dpnegf_b200 import workload
+    dev = workload.random_device(n, 3, seed=seed)
+    one = workload.BTDDevice([dev.hd[1]], [], [], [dev.sd[1]], [], [])
+    return dev, one
+
+
+def test_ozaki_equilibrium_density_matches_oracle():
+    from dpnegf_b200.density import Ozaki
+    from dpnegf_b200.device_property import DeviceProperty
+    from dpnegf_b200.lead_property import LeadProperty
+    dev, one = _single_block_setup()
+    n = dev.block_dims[1]
+    # leads couple into the single block from both sides
+    leads = {"lead_L": dev.lead_L, "lead_R": dev.lead_R}
+    ham = FakeHamiltonian(one, [1] * n, leads=leads)
+    dp = DeviceProperty(ham, None, "", e_T=300, E_ref=0.0)
+    lL = LeadProperty("lead_L", ham, None, "", voltage=0.1, efermi=0.0)
+    lR = LeadProperty("lead_R", ham, None, "", voltage=-0.1, efermi=0.0)
+    dp.set_leadLR(lL, lR)
+    oz = Ozaki(R=1e6, M_cut=20, n_gauss=6)
+    DM_eq, DM_neq = oz.integrate(dp, [0.0, 0.0, 0.0], eta_lead=1e-5, eta_device=0.0, mu=0.0,
+                                 mu_lead=lL.chemiPot_lead)
+    kBT = dp.kBT
+
+    def se(lead, z, eta):
+        hL, hLL, hDL, sL, sLL, sDL = ham.get_hs_lead([0, 0, 0], lead.tab, lead.voltage)
+        s, _, st, _ = lead_oracle.self_energy(hL.numpy(), hLL.numpy(), sL.numpy(), sLL.numpy(), z, hDL.numpy(),
+                                              sDL.numpy(), etaLead=eta, E_ref=0.0)
+        return s
+
+    def gf(z, eta=1e-5):
+        out = rgf_oracle.rgf(np.array([z]), [], [one.hd[0].numpy()], [], [one.sd[0].numpy()], [], [],
+                             se(lL, z, eta)[None], se(lR, z, eta)[None], eta=0.0)
+        return out["grd"][0][0]
+
+    def gamma_R(x):
+        s = se(lR, x, 1e-5)
+        return 1j * (s - s.conj().T)
+
+    fL = lambda x: float(lL.fermi_dirac(torch.as_tensor(float(np.real(x)), dtype=torch.float64)))
+    fR = lambda x: float(lR.fermi_dirac(torch.as_tensor(float(np.real(x)), dtype=torch.float64)))
+    ref_eq, ref_neq = lead_oracle.ozaki_density(gf, lL.chemiPot_lead, 0.0, kBT, 1e6, 20, 6, lL.voltage,
+                                                lR.voltage, fL, fR, gamma_R)
+    assert _rel(DM_eq, ref_eq) < 1e-9
+    assert _rel(DM_neq, ref_neq) < 1e-9

@@ -37,18 +37,20 @@ LESSER = 1 << 8
 DOS = 1 << 9
 ORB_GDIAG = 1 << 10
 ORB_AR = 1 << 11
+ADJOINT = 1 << 12
 PHASES = ("form", "gemm_fwd", "inv_stage", "inv_panel", "inv_update", "inv_gather", "gemm_bwd", "lesser",
           "dos", "trans", "other")
 
 # numpy mirrors of the descriptor structs (packed exactly like the C structs)
-BLOCK_FIELDS = ["hd", "sd", "hu", "su", "hl", "sl", "sdT", "suT", "slT", "orb0", "g", "o_grd", "o_grl", "o_gru", "o_grlc",
+BLOCK_FIELDS = ["hd", "sd", "hu", "su", "hl", "sl", "sdT", "suT", "slT", "orb0", "g", "gc", "gu", "o_grd", "o_grl", "o_gru",
+                "o_grlc",
                 "o_grleft", "o_gnd", "o_gnl", "o_gnu", "o_ginleft", "s_in"]
 BLOCK_DTYPE = np.dtype([("n", "<i4"), ("n_next", "<i4")] + [(f, "<i8") for f in BLOCK_FIELDS])
 DEVICE_DTYPE = np.dtype([("n_blocks", "<i4"), ("blk0", "<i4"), ("n_orb", "<i4"), ("pad", "<i4"),
                          ("o_gtrans", "<i8"), ("g_slab", "<i8")])
 ITEM_DTYPE = np.dtype([("dev", "<i4"), ("row", "<i4"), ("z_re", "<f8"), ("z_im", "<f8"),
                        ("se_l", "<u8"), ("se_r", "<u8"), ("nse_l", "<i4"), ("nse_r", "<i4"),
-                       ("out", "<i8"), ("orb", "<i8")])
+                       ("out", "<i8"), ("orb", "<i8"), ("w_t", "<f8"), ("gse_l", "<u8"), ("gse_r", "<u8")])
 
 
 LEAD_DTYPE = np.dtype([("n", "<i4"), ("nc", "<i4"), ("b", "<i4"), ("pad", "<i4"), ("h", "<i8"), ("s", "<i8"),
@@ -97,6 +99,9 @@ class NegfRgfProblem(ctypes.Structure):
         ("scratch", ctypes.c_void_p),
         ("scratch_bytes", ctypes.c_size_t),
         ("phase_cycles", ctypes.c_void_p),
+        ("grad", ctypes.c_void_p),
+        ("grad_slab", ctypes.c_int64),
+        ("col_slab", ctypes.c_int64),
     ]
 
 

@@ -33,6 +33,8 @@ constexpr int RGF_NBUF = 18;  // per-slot max_n^2 work buffers (see SlotBufs)
 struct SlotBufs {
   cplx* gslab;    // g_q storage when gr_left is not an output
   cplx* ginslab;  // lesser gin_q storage when gin_left is not an output
+  cplx* grdslab;  // adjoint: G_qq of every block (when grd is not an output)
+  cplx* colslab;  // adjoint: G_qN of every block (when gr_lc is not an output)
   cplx *W, *T1, *Lz, *Uz, *gU, *Gd, *Gl, *Gu, *Gt0, *Gt1, *tA, *tB, *tC, *tD;
   cplx *Nd, *Nl, *Nu, *tE;  // lesser work
 };
@@ -42,6 +44,7 @@ __host__ __device__ inline size_t rgf_slot_elems(const NegfRgfProblem& p) {
   size_t e = RGF_NBUF * mn2;
   if (!(p.flags & NEGF_OUT_GR_LEFT)) e += (size_t)p.max_g_slab;
   if (p.flags & NEGF_LESSER) e += (size_t)p.max_g_slab;
+  if (p.flags & NEGF_ADJOINT) e += (size_t)p.max_g_slab + (size_t)p.col_slab;
   return (e + 15) & ~(size_t)15;  // keep slots 256-byte aligned
 }
 constexpr size_t RGF_SCRATCH_HEADER = 256;  // work-queue counter
@@ -57,8 +60,14 @@ NEGF_DEV SlotBufs slot_bufs(const NegfRgfProblem& p, int slot) {
   for (int i = 0; i < RGF_NBUF; ++i) { *bufs[i] = b; b += mn2; }
   s.gslab = nullptr;
   s.ginslab = nullptr;
+  s.grdslab = nullptr;
+  s.colslab = nullptr;
   if (!(p.flags & NEGF_OUT_GR_LEFT)) { s.gslab = b; b += p.max_g_slab; }
   if (p.flags & NEGF_LESSER) { s.ginslab = b; b += p.max_g_slab; }
+  if (p.flags & NEGF_ADJOINT) {
+    s.grdslab = b; b += p.max_g_slab;
+    s.colslab = b; b += p.col_slab;
+  }
   return s;
 }
 
@@ -148,6 +157,36 @@ NEGF_DEV void gemm(cplx* smem, int M, int N, int K, const cplx* A, int64_t lda, 
   cta_gemm<OPA, OPB>(g, smem);
 }
 
+// Adjoint epilogue: W (rows of block q x cols of block p) contributes
+// dL/dX_pq = 2c W^H to the H accumulator and -2c conj(z) W^H to the S one
+// (X = H + Sigma - zS); the lead corners of the edge blocks also feed the
+// self-energy gradients.
+struct EpiGrad {
+  cplx* gH;
+  cplx* gS;
+  int ldT;       // columns of the gradient block (= rows of W)
+  double c2;     // 2 c
+  cplx zc;       // conj(z)
+  cplx* gseL;    // corner targets (null unless this W is the first / last diagonal block)
+  int cl, nsl;
+  cplx* gseR;
+  int cr, nsr, r0;  // r0 = n_N - cr
+  NEGF_DEV void operator()(int m, int n, cplx v) const {
+    const cplx h = cscale(cconj(v), c2);
+    const int64_t t = (int64_t)n * ldT + m;
+    gH[t] = cadd(gH[t], h);
+    gS[t] = csub(gS[t], cmul(zc, h));
+    if (gseL && m < cl && n < cl) {
+      cplx* d = gseL + (int64_t)n * nsl + m;
+      *d = cadd(*d, h);
+    }
+    if (gseR && m >= r0 && n >= r0) {
+      cplx* d = gseR + (int64_t)(nsr - cr + n - r0) * nsr + (nsr - cr + m - r0);
+      *d = cadd(*d, h);
+    }
+  }
+};
+
 NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBufs& sb, char* smem_raw,
                        double* red, PhaseClock& pc) {
   cplx* smem = reinterpret_cast<cplx*>(smem_raw);
@@ -218,7 +257,8 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
 
   // ----------------------------------------------------------- backward sweep
   const int nN = blk[K - 1].n;
-  const bool need_gt = (fl & (NEGF_OUT_GTRANS | NEGF_OUT_GR_LC | NEGF_TRANS | NEGF_ORB_AR)) != 0;
+  const bool adj = (fl & NEGF_ADJOINT) != 0;
+  const bool need_gt = (fl & (NEGF_OUT_GTRANS | NEGF_OUT_GR_LC | NEGF_TRANS | NEGF_ORB_AR | NEGF_ADJOINT)) != 0;
   cplx* orbg = (fl & NEGF_ORB_GDIAG) ? reinterpret_cast<cplx*>(P.orb_g) + it.orb : nullptr;
   double* orbar = ((fl & NEGF_ORB_AR) && seR) ? P.orb_ar + it.orb : nullptr;
   const int crA = seR ? min(nN, it.nse_r) : 0;
@@ -291,14 +331,15 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
     const cplx* g = gptr(q);
     cplx* grl = (fl & NEGF_OUT_GRL) ? out + b.o_grl + row * szu : sb.Gl;
     cplx* gru = (fl & NEGF_OUT_GRU) ? out + b.o_gru + row * szu : sb.Gu;
-    cplx* grd = (fl & NEGF_OUT_GRD) ? out + b.o_grd + row * sq(q) : sb.Gd;
+    cplx* grd = (fl & NEGF_OUT_GRD) ? out + b.o_grd + row * sq(q) : (adj ? sb.grdslab + b.g : sb.Gd);
     gemm<OP_N, OP_N>(smem, nq, nn, nq, g, nq, sb.Uz, nn, sb.gU, nn);         // gU = g U
     gemm<OP_N, OP_N>(smem, nn, nq, nn, Gnext, nn, sb.Lz, nq, sb.T1, nq);     // G_{q+1,q+1} L
     gemm<OP_N, OP_N>(smem, nn, nq, nq, sb.T1, nq, g, nq, grl, nq);           // grl
     gemm<OP_N, OP_N>(smem, nq, nn, nn, sb.gU, nn, Gnext, nn, gru, nn);       // gru
     gemm<OP_N, OP_N>(smem, nq, nq, nn, sb.gU, nn, grl, nq, grd, nq, ONE, g, nq);  // grd
     if (need_gt) {
-      cplx* gtn = (fl & NEGF_OUT_GR_LC) ? out + b.o_grlc + row * (int64_t)nq * nN : (tog ? sb.Gt1 : sb.Gt0);
+      cplx* gtn = (fl & NEGF_OUT_GR_LC) ? out + b.o_grlc + row * (int64_t)nq * nN
+                                          : (adj ? sb.colslab + b.gc : (tog ? sb.Gt1 : sb.Gt0));
       gemm<OP_N, OP_N>(smem, nq, nN, nn, sb.gU, nn, gt, nN, gtn, nN);
       gt = gtn;
       tog ^= 1;
@@ -375,6 +416,109 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
     }
     tval = cta_sum(part, red);
   }
+  // ------------------------------------------------------------ adjoint
+  // d(c T)/dX_pq = 2c W_qp^H with W_qp = G_qN M G_1p, M = Gamma_R G_1N^H Gamma_L
+  // restricted to the lead corners: W_qp = R_q (M_c F_p), R_q = G_qN[:, nN-cr:],
+  // F_p = G_1p[0:cl, :] = P_p G_pp, P_{p+1} = P_p g_p U_p, P_0 = I (rows 0..cl).
+  if (adj && seL && seR) {
+    const int n0 = blk[0].n;
+    const int cl = min(n0, it.nse_l), cr = min(nN, it.nse_r);
+    const double c2 = 2.0 * it.w_t;
+    const cplx zc = cconj(z);
+    const int64_t u_slab = (P.grad_slab - 2 * dv.g_slab) / 4;
+    cplx* gslot = reinterpret_cast<cplx*>(P.grad) + (size_t)blockIdx.x * P.grad_slab;
+    cplx* gHd = gslot;
+    cplx* gSd = gslot + dv.g_slab;
+    cplx* gHu = gslot + 2 * dv.g_slab;
+    cplx* gSu = gHu + u_slab;
+    cplx* gHl = gSu + u_slab;
+    cplx* gSl = gHl + u_slab;
+    const cplx* Gc = gt + (nN - cr);  // G_1N[0:cl, nN-cr:], row stride nN
+    cplx* Mc = sb.tE;                 // cr x cl
+    gemm<OP_N, OP_C>(smem, cr, cl, cr, sb.tB, cr, Gc, nN, sb.T1, cl);   // Gamma_R Gc^H
+    gemm<OP_N, OP_N>(smem, cr, cl, cl, sb.T1, cl, sb.tA, cl, Mc, cl);   // ... Gamma_L
+    // explicit Gamma terms: dT/dSigma_L = -2i K, K = Gc Gamma_R Gc^H; dT/dSigma_R = -2i Gc^H Gamma_L Gc
+    cplx* gseL = reinterpret_cast<cplx*>(it.gse_l);
+    cplx* gseR = reinterpret_cast<cplx*>(it.gse_r);
+    if (gseL) {
+      gemm<OP_N, OP_N>(smem, cl, cl, cr, Gc, nN, sb.T1, cl, sb.Nd, cl);
+      const int ns = it.nse_l;
+      for (int e = threadIdx.x; e < ns * ns; e += CTA_THREADS) {
+        int i = e / ns, j = e % ns;
+        cplx v = cmk(0.0, 0.0);
+        if (i < cl && j < cl) {
+          cplx k = sb.Nd[(int64_t)i * cl + j];
+          v = cmk(c2 * k.y, -c2 * k.x);  // -2ic k
+        }
+        gseL[e] = v;
+      }
+    }
+    if (gseR) {
+      gemm<OP_C, OP_N>(smem, cr, cr, cl, Gc, nN, sb.tC, cr, sb.Nl, cr);  // Gc^H (Gamma_L Gc)
+      const int ns = it.nse_r, o = ns - cr;
+      for (int e = threadIdx.x; e < ns * ns; e += CTA_THREADS) {
+        int i = e / ns, j = e % ns;
+        cplx v = cmk(0.0, 0.0);
+        if (i >= o && j >= o) {
+          cplx k = sb.Nl[(int64_t)(i - o) * cr + (j - o)];
+          v = cmk(c2 * k.y, -c2 * k.x);
+        }
+        gseR[e] = v;
+      }
+    }
+    __syncthreads();
+    auto colp = [&](int q) -> const cplx* {
+      if (q == K - 1) return gptr(K - 1);
+      return (fl & NEGF_OUT_GR_LC) ? out + blk[q].o_grlc + row * (int64_t)blk[q].n * nN : sb.colslab + blk[q].gc;
+    };
+    auto gpp = [&](int q) -> const cplx* {
+      if (q == K - 1) return gptr(K - 1);
+      return (fl & NEGF_OUT_GRD) ? out + blk[q].o_grd + row * sq(q) : sb.grdslab + blk[q].g;
+    };
+    cplx* Pc = sb.Gl;   // cl x n_p
+    cplx* Pn = sb.Gu;
+    cplx* Ycur = sb.Gd; // cr x n_p
+    for (int p = 0; p < K; ++p) {
+      const int np = blk[p].n;
+      const cplx* F;
+      int ldF;
+      if (p == 0) { F = gpp(0); ldF = np; }
+      else {
+        gemm<OP_N, OP_N>(smem, cl, np, np, Pc, np, gpp(p), np, sb.Lz, np);
+        F = sb.Lz; ldF = np;
+      }
+      gemm<OP_N, OP_N>(smem, cr, np, cl, Mc, cl, F, ldF, Ycur, np);       // Y_p = M_c F_p
+      const cplx* Rp = colp(p) + (nN - cr);
+      {
+        GemmArgs g = gemm_args(np, np, cr, Rp, nN, Ycur, np, nullptr, 0);
+        EpiGrad e{gHd + blk[p].g, gSd + blk[p].g, np, c2, zc, p == 0 ? gseL : nullptr, cl, it.nse_l,
+                  p == K - 1 ? gseR : nullptr, cr, it.nse_r, nN - cr};
+        cta_gemm_epi<OP_N, OP_N, true>(g, smem, e);                        // W_pp
+      }
+      if (p > 0) {  // W_{p-1,p} -> d/d(hl_{p-1}, sl_{p-1})  [n_p x n_{p-1}]
+        const int nm = blk[p - 1].n;
+        GemmArgs g = gemm_args(nm, np, cr, colp(p - 1) + (nN - cr), nN, Ycur, np, nullptr, 0);
+        EpiGrad e{gHl + blk[p - 1].gu, gSl + blk[p - 1].gu, nm, c2, zc, nullptr, 0, 0, nullptr, 0, 0, 0};
+        cta_gemm_epi<OP_N, OP_N, true>(g, smem, e);
+      }
+      if (p < K - 1) {
+        const int nn = blk[p].n_next;
+        {  // W_{p+1,p} -> d/d(hu_p, su_p)  [n_p x n_{p+1}]
+          GemmArgs g = gemm_args(nn, np, cr, colp(p + 1) + (nN - cr), nN, Ycur, np, nullptr, 0);
+          EpiGrad e{gHu + blk[p].gu, gSu + blk[p].gu, nn, c2, zc, nullptr, 0, 0, nullptr, 0, 0, 0};
+          cta_gemm_epi<OP_N, OP_N, true>(g, smem, e);
+        }
+        // P_{p+1} = P_p g_p U_p
+        form_shift(sb.Uz, hs, blk[p].hu, blk[p].su, z, np, nn, smem);
+        gemm<OP_N, OP_N>(smem, np, nn, np, gptr(p), np, sb.Uz, nn, sb.gU, nn);
+        if (p == 0) copy_mat(Pn, sb.gU, cl, nn, smem);
+        else gemm<OP_N, OP_N>(smem, cl, nn, np, Pc, np, sb.gU, nn, Pn, nn);
+        cplx* t = Pc; Pc = Pn; Pn = t;
+      }
+    }
+    pc.mark(PH_GEMM_BWD);
+  }
+
   if (threadIdx.x == 0) {
     if (fl & NEGF_TRANS) P.trans[it.out] = tval;
     if (fl & NEGF_DOS) P.dos[it.out] = dos_total;
@@ -439,6 +583,9 @@ int negf_rgf_run(const NegfRgfProblem* p, void* stream) {
   if ((p->flags & NEGF_DOS) && !p->dos) return NEGF_ERR_ARGUMENT;
   if ((p->flags & NEGF_ORB_GDIAG) && !p->orb_g) return NEGF_ERR_ARGUMENT;
   if ((p->flags & NEGF_ORB_AR) && !p->orb_ar) return NEGF_ERR_ARGUMENT;
+  if ((p->flags & NEGF_ADJOINT) &&
+      (!p->grad || p->grad_slab <= 0 || p->col_slab <= 0 || !(p->flags & NEGF_TRANS)))
+    return NEGF_ERR_ARGUMENT;
   const uint32_t blockouts = NEGF_OUT_GTRANS | NEGF_OUT_GR_LC | NEGF_OUT_GRD | NEGF_OUT_GRL | NEGF_OUT_GRU |
                              NEGF_OUT_GR_LEFT | NEGF_LESSER;
   if ((p->flags & blockouts) && !p->out) return NEGF_ERR_ARGUMENT;

@@ -66,6 +66,8 @@ class Geometry:
             blk0 = len(blocks)
             g = 0
             orb = 0
+            gc = 0
+            gu = 0
             for q in range(K):
                 n = dims[q]
                 if tuple(d.hd[q].shape[-2:]) != (n, n) or tuple(d.sd[q].shape[-2:]) != (n, n):
@@ -92,6 +94,11 @@ class Geometry:
                         offdiag.append((len(blocks), name, int(b[name]), t.numel()))
                 b["orb0"] = orb
                 b["g"] = g
+                b["gc"] = gc
+                b["gu"] = gu
+                gc += n * dims[-1]
+                if q + 1 < K:
+                    gu += n * dims[q + 1]
                 for f in ("o_grd", "o_grl", "o_gru", "o_grlc", "o_grleft", "o_gnd", "o_gnl", "o_gnu",
                           "o_ginleft", "s_in"):
                     b[f] = -1
@@ -107,6 +114,8 @@ class Geometry:
             dv["g_slab"] = g
             devs.append(dv)
             self.max_g_slab = max(self.max_g_slab, g)
+            self.col_slab = max(getattr(self, "col_slab", 0), gc)
+            self.u_slab = max(getattr(self, "u_slab", 0), gu)
         if self.max_n > _lib.NEGF_MAX_BLOCK:
             raise ValueError(f"block size {self.max_n} exceeds the supported maximum {_lib.NEGF_MAX_BLOCK}")
         # one host->device copy per block straight into the arena
@@ -140,6 +149,7 @@ class RgfResult:
     phase_cycles: Optional[torch.Tensor] = None  # [n_slots, NEGF_PHASES] SM cycles per phase
     orb_g: Optional[torch.Tensor] = None    # concatenated per-item [n_orb] diag(G_qq) (complex)
     orb_ar: Optional[torch.Tensor] = None   # concatenated per-item [n_orb] diag(G_qN Gamma_R G_qN^H)
+    grads: Optional[dict] = None            # adjoint: block gradients and per-energy dT/dSigma
 
 
 _FAMILY = {  # output tag -> (flag, block field, shape fn (n_q, n_next, n_last))
@@ -159,7 +169,7 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
         se_r: List[Optional[torch.Tensor]], eta=0.0, E_ref=0.0, outputs=("g_trans", "grd", "grl", "gru"),
         trans=False, orb_dos=False, dos=False, orb_g=False, orb_ar=False,
         s_in: Optional[List[List[Optional[torch.Tensor]]]] = None,
-        n_slots=None, check=True, stream=None, phase=False, events=None):
+        n_slots=None, check=True, stream=None, phase=False, events=None, adjoint_w=None):
     """Run the batched sweep.
 
     ``energies[d]`` is a 1-D tensor of B_d energies for device d; ``se_l[d]``
@@ -169,6 +179,9 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     (None entries are zero blocks) and switches the lesser sweep on.
     ``events=(start, end)`` are CUDA events recorded on the launch stream
     immediately around the kernel (device time of the sweep alone).
+    ``adjoint_w`` ([B] weights of T(E), single device) switches the adjoint
+    on: the result carries d(sum w T)/d(hd, hu, hl, sd, su, sl) and per-energy
+    dT/dSigma_L, dT/dSigma_R weighted by w (torch's complex convention).
     """
     _lib.require_cuda()
     lib = _lib.load()
@@ -198,6 +211,12 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
         flags |= _lib.ORB_AR
     if lesser:
         flags |= _lib.LESSER
+    adjoint = adjoint_w is not None
+    if adjoint:
+        if nd != 1:
+            raise ValueError("the adjoint runs on a single device")
+        flags |= _lib.ADJOINT | _lib.TRANS
+        trans = True
 
     blocks = geom.blocks.copy()
     devs = geom.devs.copy()
@@ -270,6 +289,14 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
         n_orb = int(devs[d]["n_orb"])
         rows = np.arange(B, dtype=np.int64)
         it = np.zeros(B, dtype=_lib.ITEM_DTYPE)
+        if adjoint:
+            w = torch.as_tensor(adjoint_w, dtype=torch.float64).reshape(-1).cpu().numpy()
+            it["w_t"] = w
+            gseL_t = torch.empty((B, nsl, nsl), dtype=C128, device=dev) if nsl else None
+            gseR_t = torch.empty((B, nsr, nsr), dtype=C128, device=dev) if nsr else None
+            keep_alive += [x for x in (gseL_t, gseR_t) if x is not None]
+            it["gse_l"] = (gseL_t.data_ptr() + rows * nsl * nsl * 16) if nsl else 0
+            it["gse_r"] = (gseR_t.data_ptr() + rows * nsr * nsr * 16) if nsr else 0
         it["dev"] = d
         it["row"] = rows
         it["z_re"] = z.real
@@ -328,6 +355,19 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     scratch = torch.empty(max(need, 256), dtype=torch.uint8, device=dev)
     prob.scratch = scratch.data_ptr()
     prob.scratch_bytes = scratch.numel()
+    grad_t = None
+    if adjoint:
+        g_slab = int(geom.devs[0]["g_slab"])
+        grad_slab = 2 * g_slab + 4 * int(geom.u_slab)
+        grad_t = torch.zeros((n_slots, max(grad_slab, 1)), dtype=C128, device=dev)
+        prob.grad = grad_t.data_ptr()
+        prob.grad_slab = grad_slab
+        prob.col_slab = max(int(geom.col_slab), 1)
+        need = lib.negf_rgf_scratch_bytes(ctypes.byref(prob))
+        if need > scratch.numel():
+            scratch = torch.empty(need, dtype=torch.uint8, device=dev)
+            prob.scratch = scratch.data_ptr()
+            prob.scratch_bytes = scratch.numel()
     phase_t = None
     if phase:
         phase_t = torch.zeros((n_slots, len(_lib.PHASES)), dtype=torch.int64, device=dev)
@@ -360,9 +400,30 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
                 raise torch.linalg.LinAlgError(
                     f"RGF: a left-connected block is singular (item {bad}); the matrix is not invertible")
             raise _lib.NegfError(f"RGF failed for item {bad} with status {code}")
+    grads = None
+    if adjoint:
+        gsum = grad_t.sum(0)
+        K = int(geom.devs[0]["n_blocks"])
+        dims = [int(geom.blocks[q]["n"]) for q in range(K)]
+        g_slab = int(geom.devs[0]["g_slab"])
+        u_slab = int(geom.u_slab)
+        base = {"hd": 0, "sd": g_slab, "hu": 2 * g_slab, "su": 2 * g_slab + u_slab,
+                "hl": 2 * g_slab + 2 * u_slab, "sl": 2 * g_slab + 3 * u_slab}
+        grads = {}
+        for name in ("hd", "sd"):
+            grads[name] = [gsum[base[name] + int(geom.blocks[q]["g"]):][:dims[q] ** 2].view(dims[q], dims[q])
+                           for q in range(K)]
+        for name in ("hu", "su"):
+            grads[name] = [gsum[base[name] + int(geom.blocks[q]["gu"]):][:dims[q] * dims[q + 1]]
+                           .view(dims[q], dims[q + 1]) for q in range(K - 1)]
+        for name in ("hl", "sl"):
+            grads[name] = [gsum[base[name] + int(geom.blocks[q]["gu"]):][:dims[q] * dims[q + 1]]
+                           .view(dims[q + 1], dims[q]) for q in range(K - 1)]
+        grads["se_l"] = gseL_t
+        grads["se_r"] = gseR_t
     return RgfResult(trans=trans_t[:item_cursor] if trans else None,
                      orb_dos=orb_t[:orb_cursor] if orb_dos else None,
                      dos=dos_t[:item_cursor] if dos else None,
                      status=status_t[:item_cursor], blocks=res_blocks, phase_cycles=phase_t,
                      orb_g=orbg_t[:orb_cursor] if orb_g else None,
-                     orb_ar=orbar_t[:orb_cursor] if orb_ar else None)
+                     orb_ar=orbar_t[:orb_cursor] if orb_ar else None, grads=grads)

@@ -56,6 +56,7 @@ extern "C" {
 #define NEGF_DOS (1u << 9)         /* DOS = 2 sum_i (-Im diag(G S)_i / pi) -> dos[]  */
 #define NEGF_ORB_GDIAG (1u << 10)  /* diag(G_qq) per orbital (complex128)  -> orb_g[] */
 #define NEGF_ORB_AR (1u << 11)     /* diag(G_qN Gamma_R G_qN^H) per orbital -> orb_ar[] */
+#define NEGF_ADJOINT (1u << 12)    /* accumulate d(sum_items w_T T)/d(H, S) and dT/dSigma (single device) */
 
 /* Phase indices of NegfRgfProblem.phase_cycles (clock64 cycles per slot). */
 #define NEGF_PHASES 11 /* form, gemm_fwd, inv_stage, inv_panel, inv_update, inv_gather,
@@ -72,6 +73,8 @@ typedef struct NegfBlock {
                             the DOS diagonals; -1 = zero block */
   int64_t orb0;   /* first orbital of block q within its device */
   int64_t g;      /* offset of g_q inside one item's g slab (prefix sum of n^2) */
+  int64_t gc;     /* NEGF_ADJOINT: offset of G_qN in the per-slot column slab (prefix of n_q n_N) */
+  int64_t gu;     /* NEGF_ADJOINT: offset of the coupling gradients of block q (prefix of n_q n_{q+1}) */
   /* block outputs: offset of batch row 0 in out; row b adds b * (block size).
      -1 when not produced. */
   int64_t o_grd, o_grl, o_gru, o_grlc, o_grleft;
@@ -100,6 +103,9 @@ typedef struct NegfItem {
   int32_t nse_l, nse_r;
   int64_t out;     /* index into trans[] and status[] */
   int64_t orb;     /* offset (doubles) of this item's n_orb entries in orb_dos[] */
+  double w_t;      /* NEGF_ADJOINT: weight of this item's T(E) in the loss */
+  double* gse_l;   /* NEGF_ADJOINT: d loss / d Sigma_L [nse_l x nse_l] (torch convention); NULL = skip */
+  double* gse_r;   /* NEGF_ADJOINT: d loss / d Sigma_R [nse_r x nse_r]; NULL = skip */
 } NegfItem;
 
 typedef struct NegfRgfProblem {
@@ -123,6 +129,13 @@ typedef struct NegfRgfProblem {
   void* scratch;            /* >= negf_rgf_scratch_bytes(problem) bytes, 256-aligned */
   size_t scratch_bytes;
   unsigned long long* phase_cycles; /* optional [n_slots x NEGF_PHASES] SM-cycle counters; NULL = off */
+  /* NEGF_ADJOINT: per-slot gradient accumulators, complex128, [n_slots x grad_slab]; the caller
+     zeroes them and sums over slots.  Within a slot: d/dhd, d/dsd at g offsets (g_slab each),
+     then d/dhu, d/dsu, d/dhl, d/dsl at gu offsets (u_slab = sum n_q n_{q+1} each).
+     Gradients follow torch's convention for complex inputs: dL/dRe + i dL/dIm. */
+  double* grad;
+  int64_t grad_slab;        /* complex elements per slot: 2 g_slab + 4 u_slab */
+  int64_t col_slab;         /* NEGF_ADJOINT: sum_q n_q n_N (last-column slab per slot) */
 } NegfRgfProblem;
 
 /* ---- Lopez-Sancho lead decimation ------------------------------------ */

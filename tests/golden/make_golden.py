@@ -16,7 +16,10 @@ seeded inputs together with the reference's own outputs:
   lopez_*.npz     ``surface_green`` / ``selfEnergy`` (negf/surface_green.py)
                   for the 1-D chain lead and a random non-orthogonal lead;
   ozaki.npz       ``ozaki_residues`` (negf/ozaki_res_cal.py) and ``gauss_xw``
-                  (negf/negf_utils.py:136).
+                  (negf/negf_utils.py:136);
+  adjoint_*.npz   gradients of sum_E w_E T(E) w.r.t. every H/S block and both
+                  self-energies by torch autograd through the reference
+                  ``recursive_gf`` (T as in ``_cal_tc_``, device_property.py:374-406).
 The fixtures are small (tens of KB) and are committed; the GPU box never needs
 the reference sources.
 """
@@ -219,9 +222,40 @@ def _ozaki_cases(oz_mod, nu_mod):
     np.savez_compressed(os.path.join(HERE, "ozaki.npz"), **d)
 
 
+def _adjoint_case(rgf_mod, name, dims, B, seed, eta=1e-5):
+    dev = workload.random_device(0, 0, seed=seed, block_dims=dims)
+    leaf = lambda xs: [x.clone().requires_grad_(True) for x in xs]
+    hd, hu, hl, sd, su, sl = (leaf(getattr(dev, k)) for k in ("hd", "hu", "hl", "sd", "su", "sl"))
+    seL = workload.random_self_energy(B, dims[0], seed=seed + 1).requires_grad_(True)
+    seR = workload.random_self_energy(B, dims[-1], seed=seed + 2).requires_grad_(True)
+    E = torch.linspace(-1.2, 1.3, B, dtype=torch.float64).to(torch.complex128)
+    w = torch.linspace(0.5, 1.5, B, dtype=torch.float64)
+    ans = rgf_mod.recursive_gf(E, hl=hl, hd=hd, hu=hu, sd=sd, su=su, sl=sl, left_se=seL, right_se=seR, eta=eta)
+    G = ans[0]
+    gL = 1j * (seL - seL.mH)
+    gR = 1j * (seR - seR.mH)
+    T = (gL @ G @ gR @ G.mH).diagonal(dim1=-2, dim2=-1).real.sum(-1)
+    (w * T).sum().backward()
+    d = {}
+    _put(d, "dims", np.array(dims))
+    _put(d, "energy", E)
+    _put(d, "eta", np.array(eta))
+    _put(d, "w", w)
+    _put(d, "T", T.detach())
+    for k, v in (("hd", hd), ("hu", hu), ("hl", hl), ("sd", sd), ("su", su), ("sl", sl)):
+        _put(d, k, [x.detach() for x in v])
+        _put(d, "grad/" + k, [x.grad for x in v])
+    _put(d, "left_se", seL.detach())
+    _put(d, "right_se", seR.detach())
+    _put(d, "grad/left_se", seL.grad)
+    _put(d, "grad/right_se", seR.grad)
+    np.savez_compressed(os.path.join(HERE, f"adjoint_{name}.npz"), **d)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default=ref_import.DEFAULT_REF_ROOT)
+    ap.add_argument("--only", default=None, help="regenerate one family: rgf, devprop, lopez, ozaki, adjoint")
     args = ap.parse_args()
     torch.set_num_threads(1)  # the container's threaded batched zgesv can hang
     rgf_mod = ref_import.load("recursive_green_cal", args.ref_root)
@@ -230,18 +264,27 @@ def main():
     oz_mod = ref_import.load("ozaki_res_cal", args.ref_root)
     nu_mod = ref_import.load("negf_utils", args.ref_root)
 
-    _rgf_case(rgf_mod, "nonuniform_retarded", [8, 6, 8], 6, seed=1)
-    _rgf_case(rgf_mod, "uniform_retarded", [8] * 5, 6, seed=2, E_ref=0.1)
-    _rgf_case(rgf_mod, "uniform_lesser", [6] * 4, 4, seed=3, lesser=True)
-    _rgf_case(rgf_mod, "nonuniform_lesser", [5, 7, 4], 3, seed=4, lesser=True)
-    _rgf_case(rgf_mod, "scalar_retarded", [4, 4, 4], 1, seed=5, scalar=True)
-    _rgf_case(rgf_mod, "greater", [4, 5, 4], 3, seed=6, greater=True, lesser=True)
-    _rgf_case(rgf_mod, "two_blocks", [3, 3], 2, seed=8)
-    _rgf_case(rgf_mod, "wide_uniform", [20] * 4, 2, seed=9, gr_lc=False)
-    _devprop_case(dp_mod, "nonuniform", [4, 5, 4], 5, seed=10, norbs=[2, 3, 1, 3, 4])
-    _devprop_case(dp_mod, "uniform", [6] * 4, 4, seed=11, norbs=[1] * 24)
-    _lopez_cases(sg_mod)
-    _ozaki_cases(oz_mod, nu_mod)
+    want = lambda fam: args.only in (None, fam)
+    if want("rgf"):
+        _rgf_case(rgf_mod, "nonuniform_retarded", [8, 6, 8], 6, seed=1)
+        _rgf_case(rgf_mod, "uniform_retarded", [8] * 5, 6, seed=2, E_ref=0.1)
+        _rgf_case(rgf_mod, "uniform_lesser", [6] * 4, 4, seed=3, lesser=True)
+        _rgf_case(rgf_mod, "nonuniform_lesser", [5, 7, 4], 3, seed=4, lesser=True)
+        _rgf_case(rgf_mod, "scalar_retarded", [4, 4, 4], 1, seed=5, scalar=True)
+        _rgf_case(rgf_mod, "greater", [4, 5, 4], 3, seed=6, greater=True, lesser=True)
+        _rgf_case(rgf_mod, "two_blocks", [3, 3], 2, seed=8)
+        _rgf_case(rgf_mod, "wide_uniform", [20] * 4, 2, seed=9, gr_lc=False)
+    if want("devprop"):
+        _devprop_case(dp_mod, "nonuniform", [4, 5, 4], 5, seed=10, norbs=[2, 3, 1, 3, 4])
+        _devprop_case(dp_mod, "uniform", [6] * 4, 4, seed=11, norbs=[1] * 24)
+    if want("lopez"):
+        _lopez_cases(sg_mod)
+    if want("ozaki"):
+        _ozaki_cases(oz_mod, nu_mod)
+    if want("adjoint"):
+        _adjoint_case(rgf_mod, "nonuniform", [6, 9, 5, 7], 3, seed=21)
+        _adjoint_case(rgf_mod, "uniform", [10] * 5, 2, seed=22)
+        _adjoint_case(rgf_mod, "single_block", [8], 2, seed=23)
     print("golden fixtures written to", HERE)
 
 

@@ -1,0 +1,123 @@
+"""Adjoint RGF on the GPU: gradients of sum_E w_E T(E) against torch autograd
+through the reference recursive_gf (fixtures) and central finite differences
+of the CUDA forward sweep."""
+import numpy as np
+import pytest
+import torch
+
+from tests.goldens import Golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    a = a.detach().cpu().numpy() if torch.is_tensor(a) else np.asarray(a)
+    b = np.asarray(b)
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def _inputs(g):
+    cu = lambda xs: [torch.as_tensor(x).cuda().requires_grad_(True) for x in xs]
+    blocks = {k: cu(g[k]) for k in ("hd", "hu", "hl", "sd", "su", "sl")}
+    seL = torch.as_tensor(g["left_se"]).cuda().requires_grad_(True)
+    seR = torch.as_tensor(g["right_se"]).cuda().requires_grad_(True)
+    return blocks, seL, seR
+
+
+@pytest.mark.parametrize("case", ["adjoint_nonuniform", "adjoint_uniform", "adjoint_single_block"])
+def test_gradients_match_reference_autograd(case):
+    from dpnegf_b200.adjoint import transmission
+    g = Golden(case)
+    b, seL, seR = _inputs(g)
+    E = torch.as_tensor(g["energy"]).cuda()
+    T = transmission(b["hd"], b["hu"], b["hl"], b["sd"], b["su"], b["sl"], E, seL, seR, eta=float(g["eta"]))
+    assert _rel(T, g["T"]) < 1e-10
+    w = torch.as_tensor(g["w"]).cuda()
+    (w * T).sum().backward()
+    for k in ("hd", "hu", "hl", "sd", "su", "sl"):
+        for q, (x, ref) in enumerate(zip(b[k], g["grad/" + k])):
+            assert _rel(x.grad, ref) < 1e-9, (k, q, _rel(x.grad, ref))
+    assert _rel(seL.grad, g["grad/left_se"]) < 1e-9
+    assert _rel(seR.grad, g["grad/right_se"]) < 1e-9
+
+
+def test_gradients_match_finite_differences():
+    """Central differences (h = 1e-6) of the CUDA forward on random entries."""
+    from dpnegf_b200 import workload
+    from dpnegf_b200.adjoint import transmission
+    dims = [12, 16, 12]
+    dev = workload.random_device(0, 0, seed=5, block_dims=dims)
+    B = 3
+    seL = workload.random_self_energy(B, dims[0], seed=6).cuda()
+    seR = workload.random_self_energy(B, dims[-1], seed=7).cuda()
+    E = torch.tensor([-0.7, 0.1, 0.9], dtype=torch.complex128).cuda()
+    w = torch.tensor([1.0, -0.5, 2.0], dtype=torch.float64).cuda()
+    blocks = {k: [x.cuda().requires_grad_(True) for x in getattr(dev, k)] for k in ("hd", "hu", "hl", "sd", "su", "sl")}
+    seLr = seL.clone().requires_grad_(True)
+    seRr = seR.clone().requires_grad_(True)
+
+    def loss(bl, sL, sR):
+        T = transmission(bl["hd"], bl["hu"], bl["hl"], bl["sd"], bl["su"], bl["sl"], E, sL, sR, eta=1e-5)
+        return (w * T).sum()
+
+    loss(blocks, seLr, seRr).backward()
+    rng = np.random.default_rng(0)
+    h = 1e-6
+    checks = [("hd", 1), ("hu", 0), ("hl", 1), ("sd", 2), ("su", 1), ("sl", 0)]
+    with torch.no_grad():
+        base = {k: [x.detach().clone() for x in v] for k, v in blocks.items()}
+        for name, q in checks:
+            X = base[name][q]
+            for _ in range(3):
+                i, j = rng.integers(X.shape[0]), rng.integers(X.shape[1])
+                for part, unit in (("re", 1.0), ("im", 1j)):
+                    def shifted(s):
+                        bl = {k: [x.clone() for x in v] for k, v in base.items()}
+                        bl[name][q][i, j] += s * unit
+                        return loss(bl, seL, seR).item()
+                    fd = (shifted(h) - shifted(-h)) / (2 * h)
+                    gr = blocks[name][q].grad[i, j]
+                    ad = gr.real.item() if part == "re" else gr.imag.item()
+                    assert abs(fd - ad) <= 1e-6 * max(1.0, abs(ad)), (name, q, i, j, part, fd, ad)
+        for which, S, gradS in (("L", seL, seLr.grad), ("R", seR, seRr.grad)):
+            for _ in range(3):
+                e, i, j = rng.integers(B), rng.integers(S.shape[1]), rng.integers(S.shape[2])
+                for part, unit in (("re", 1.0), ("im", 1j)):
+                    def shifted(s):
+                        S2 = S.clone()
+                        S2[e, i, j] += s * unit
+                        return loss(base, S2, seR).item() if which == "L" else loss(base, seL, S2).item()
+                    fd = (shifted(h) - shifted(-h)) / (2 * h)
+                    gr = gradS[e, i, j]
+                    ad = gr.real.item() if part == "re" else gr.imag.item()
+                    assert abs(fd - ad) <= 1e-6 * max(1.0, abs(ad)), (which, e, i, j, part, fd, ad)
+
+
+def test_current_gradient_chains_through_simpson():
+    from dpnegf_b200 import workload
+    from dpnegf_b200.adjoint import current, transmission
+    dims = [10, 10, 10]
+    dev = workload.random_device(0, 0, seed=9, block_dims=dims)
+    n_e = 9
+    E = torch.linspace(-0.3, 0.3, n_e, dtype=torch.float64)
+    seL = workload.random_self_energy(n_e, 10, seed=1).cuda()
+    seR = workload.random_self_energy(n_e, 10, seed=2).cuda()
+    hd1 = dev.hd[1].cuda().requires_grad_(True)
+    blocks = [x.cuda() for x in dev.hd]
+    kT = 0.025
+    fL = 1 / (1 + torch.exp((E - 0.15) / kT))
+    fR = 1 / (1 + torch.exp((E + 0.15) / kT))
+
+    def I(h1):
+        T = transmission([blocks[0], h1, blocks[2]], [x.cuda() for x in dev.hu], [x.cuda() for x in dev.hl],
+                         [x.cuda() for x in dev.sd], [x.cuda() for x in dev.su], [x.cuda() for x in dev.sl],
+                         E.to(torch.complex128).cuda(), seL, seR, eta=1e-5)
+        return current(T, E.cuda(), fL.cuda(), fR.cuda())
+
+    I(hd1).backward()
+    with torch.no_grad():
+        h = 1e-6
+        d = torch.zeros_like(hd1)
+        d[2, 3] = h
+        fd = (I(hd1.detach() + d) - I(hd1.detach() - d)).item() / (2 * h)
+    assert abs(fd - hd1.grad[2, 3].real.item()) <= 1e-6 * max(1.0, abs(fd))

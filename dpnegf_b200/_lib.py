@@ -19,6 +19,7 @@ NEGF_ERR_LS_NOT_CONVERGED = 2
 NEGF_ERR_LS_RESIDUAL = 3
 NEGF_ERR_SINGULAR = 4
 NEGF_ERR_NONFINITE = 5
+NEGF_ERR_TIMEOUT = 6
 NEGF_ERR_ARGUMENT = -1
 NEGF_ERR_UNSUPPORTED = -2
 NEGF_ERR_CUDA = -3
@@ -38,8 +39,10 @@ DOS = 1 << 9
 ORB_GDIAG = 1 << 10
 ORB_AR = 1 << 11
 ADJOINT = 1 << 12
+MIXED = 1 << 13
+REFINE = 1 << 14
 PHASES = ("form", "gemm_fwd", "inv_stage", "inv_panel", "inv_update", "inv_gather", "gemm_bwd", "lesser",
-          "dos", "trans", "other")
+          "dos", "trans", "other", "refine")
 
 # numpy mirrors of the descriptor structs (packed exactly like the C structs)
 BLOCK_FIELDS = ["hd", "sd", "hu", "su", "hl", "sl", "sdT", "suT", "slT", "orb0", "g", "gc", "gu", "o_grd", "o_grl", "o_gru",
@@ -102,6 +105,8 @@ class NegfRgfProblem(ctypes.Structure):
         ("grad", ctypes.c_void_p),
         ("grad_slab", ctypes.c_int64),
         ("col_slab", ctypes.c_int64),
+        ("refine_steps", ctypes.c_int32),
+        ("pad2", ctypes.c_int32),
     ]
 
 

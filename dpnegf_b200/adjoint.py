@@ -29,13 +29,14 @@ from .negf_utils import simpson
 
 class _TransmissionFn(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, energy, eta, E_ref, K, left_se, right_se, *blocks):
+    def forward(ctx, energy, eta, E_ref, K, precision, refine, left_se, right_se, *blocks):
         hd, hu, hl, sd, su, sl = _split(blocks, K)
         geom = rgf_plan.Geometry([rgf_plan.DeviceBlocks(hd, hu, hl, sd, su, sl)], device=left_se.device,
                                  detect_zero_offdiag=False)
-        res = rgf_plan.run(geom, [energy], [left_se], [right_se], eta=eta, E_ref=E_ref, outputs=(), trans=True)
+        res = rgf_plan.run(geom, [energy], [left_se], [right_se], eta=eta, E_ref=E_ref, outputs=(), trans=True,
+                           precision=precision, refine=refine)
         ctx.geom = geom
-        ctx.eta, ctx.E_ref, ctx.K = eta, E_ref, K
+        ctx.eta, ctx.E_ref, ctx.K, ctx.precision = eta, E_ref, K, precision
         ctx.save_for_backward(energy, left_se, right_se)
         return res.trans.clone()
 
@@ -43,12 +44,12 @@ class _TransmissionFn(torch.autograd.Function):
     def backward(ctx, gT):
         energy, left_se, right_se = ctx.saved_tensors
         res = rgf_plan.run(ctx.geom, [energy], [left_se], [right_se], eta=ctx.eta, E_ref=ctx.E_ref, outputs=(),
-                           adjoint_w=gT.detach().to(torch.float64))
+                           adjoint_w=gT.detach().to(torch.float64), precision=ctx.precision)
         g = res.grads
         K = ctx.K
         block_grads = g["hd"] + g["hu"] + g["hl"] + g["sd"] + g["su"] + g["sl"]
         assert len(block_grads) == 6 * K - 4
-        return (None, None, None, None, g["se_l"], g["se_r"]) + tuple(block_grads)
+        return (None, None, None, None, None, None, g["se_l"], g["se_r"]) + tuple(block_grads)
 
 
 def _split(blocks, K):
@@ -64,15 +65,20 @@ def _split(blocks, K):
 def transmission(hd: Sequence[torch.Tensor], hu: Sequence[torch.Tensor], hl: Sequence[torch.Tensor],
                  sd: Sequence[torch.Tensor], su: Sequence[torch.Tensor], sl: Sequence[torch.Tensor],
                  energy: torch.Tensor, left_se: torch.Tensor, right_se: torch.Tensor, eta: float = 0.0,
-                 E_ref: float = 0.0) -> torch.Tensor:
+                 E_ref: float = 0.0, precision: str = "fp64", refine: bool = False) -> torch.Tensor:
     """T(E) [B] of one BTD device, differentiable w.r.t. every 2-D block and both
-    ``[B, n, n]`` self-energies (CUDA tensors)."""
+    ``[B, n, n]`` self-energies (CUDA tensors).
+
+    ``precision="mixed"`` runs the forward sweep and the adjoint pass on the
+    tcgen05 3xTF32 products (gradients at FP32-product accuracy); ``refine``
+    refines the forward T(E) with an FP64 residual."""
     K = len(hd)
     if not (len(sd) == K and len(hu) == len(hl) == len(su) == len(sl) == K - 1):
         raise ValueError("inconsistent block lists")
     energy = torch.as_tensor(energy).to(torch.complex128).reshape(-1).detach()
     blocks = list(hd) + list(hu) + list(hl) + list(sd) + list(su) + list(sl)
-    return _TransmissionFn.apply(energy, float(eta), float(E_ref), K, left_se, right_se, *blocks)
+    return _TransmissionFn.apply(energy, float(eta), float(E_ref), K, precision, bool(refine), left_se, right_se,
+                                 *blocks)
 
 
 def current(T: torch.Tensor, energy: torch.Tensor, f_left: torch.Tensor, f_right: torch.Tensor) -> torch.Tensor:

@@ -28,28 +28,44 @@
 // pivot search for the next column uses the entries each thread just
 // produced.  Two barriers per column.
 #pragma once
-#include "cta_gemm.cuh"
+#include "cta_gemm_tc.cuh"
 
 namespace negf {
 
 constexpr int INV_OB = 128;  // outer block (columns) of the two-level Gauss-Jordan
 
+// Shared memory: panel, R tiles, pivot row and multiplier columns, then the
+// integer maps (piv, pinv, reductions).  With the tensor-core outer update
+// (TC) the maps start above the tcgen05 staging area, which that GEMM
+// overwrites while the update epilogue still reads pinv.
 template <int NB>
 struct InvLayout {
   static constexpr int PP = NB + 4;  // panel pitch (= 4 mod 8: conflict-free A fragments)
   static constexpr int RP = GT_N + 2;
   __host__ __device__ static int rows(int n) { return (n + GT_M - 1) / GT_M * GT_M; }
-  __host__ __device__ static size_t bytes(int n) {
+  __host__ __device__ static size_t panel_bytes(int n) {
     size_t b = (size_t)rows(n) * PP * sizeof(double2) + 2 * (size_t)NB * RP * sizeof(double2);
-    b += 2 * (size_t)rows(n) * sizeof(double2) + NB * sizeof(double2);  // multiplier columns, spare row
-    b += (size_t)(2 * n + 64) * sizeof(int) + 16 * sizeof(double);
-    return b;
+    return b + 2 * (size_t)rows(n) * sizeof(double2) + NB * sizeof(double2);  // multiplier columns, spare row
+  }
+  __host__ __device__ static size_t maps_offset(int n, bool tc) {
+    size_t b = panel_bytes(n);
+    return (tc && b < (size_t)TC_SMEM_BYTES) ? (size_t)TC_SMEM_BYTES : b;
+  }
+  __host__ __device__ static size_t bytes(int n, bool tc) {
+    return maps_offset(n, tc) + (size_t)(2 * n + 64) * sizeof(int) + 16 * sizeof(double);
   }
 };
 
-inline size_t inv_smem_bytes_host(int n) {
-  size_t a = n <= 256 ? InvLayout<32>::bytes(n) : InvLayout<16>::bytes(n);
-  return a > (size_t)GEMM_SMEM_BYTES ? a : (size_t)GEMM_SMEM_BYTES;  // the outer update runs the tile GEMM
+// Largest footprint over every block size up to max_n: blocks up to 256 use
+// 32-wide panels, larger ones 16-wide panels, and a device may mix both.
+inline size_t inv_smem_bytes_host(int max_n, bool tc = false) {
+  size_t a = InvLayout<32>::bytes(max_n < 256 ? max_n : 256, tc);
+  if (max_n > 256) {
+    const size_t b = InvLayout<16>::bytes(max_n, tc);
+    if (b > a) a = b;
+  }
+  size_t g = tc ? (size_t)TC_SMEM_BYTES : (size_t)GEMM_SMEM_BYTES;  // the outer update runs a CTA GEMM
+  return a > g ? a : g;
 }
 
 // Complex elements of the pivot-row snapshot the inverse needs (INV_OB x n).
@@ -96,8 +112,9 @@ struct EpiGJ {
 
 // Returns 0 on success, 1 if a zero or non-finite pivot was met.  Uniform
 // across the CTA; ends with __syncthreads().  `snap` is global scratch of
-// inv_snapshot_elems(n) complex elements (unused when n <= INV_OB).
-template <int NB, int RT, bool G3>
+// inv_snapshot_elems(n) complex elements (unused when n <= INV_OB).  TC runs
+// the outer update on the tcgen05 3xTF32 GEMM (FP32-accurate products).
+template <int NB, int RT, bool G3, bool TC>
 __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G, int64_t ldg, char* smem_raw,
                                            PhaseClock* pc, cplx* snap) {
   constexpr int PP = InvLayout<NB>::PP;
@@ -108,7 +125,7 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
   cplx* P = reinterpret_cast<cplx*>(smem_raw);
   cplx* Rb[2] = {P + (size_t)n_pad * PP, P + (size_t)n_pad * PP + NB * RP};
   cplx* qrow = Rb[1] + NB * RP;  // [NB] published pivot row of the current column
-  int* piv = reinterpret_cast<int*>(qrow + 2 * n_pad + NB);  // logical column -> physical row
+  int* piv = reinterpret_cast<int*>(smem_raw + InvLayout<NB>::maps_offset(n, TC));  // logical column -> physical row
   int* pinv = piv + n;                           // physical row -> logical column (-1: unused)
   int* red_i = pinv + n;                         // [2][NWARP] pivot candidates (double buffered)
   int* s_misc = red_i + 2 * NWARP;               // [1]: singular flag
@@ -313,11 +330,13 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
       __syncthreads();
       if (c_lo > 0) {
         GemmArgs g = gemm_args(n, c_lo, kb, W + c_lo, ldw, snap, n, W, ldw);
-        cta_gemm_epi<OP_N, OP_N, G3>(g, reinterpret_cast<cplx*>(smem_raw), EpiGJ{W, ldw, pinv, c_lo, c_hi, 0});
+        if constexpr (TC) cta_gemm_tc_epi<OP_N, OP_N>(g, smem_raw, EpiGJ{W, ldw, pinv, c_lo, c_hi, 0});
+        else cta_gemm_epi<OP_N, OP_N, G3>(g, reinterpret_cast<cplx*>(smem_raw), EpiGJ{W, ldw, pinv, c_lo, c_hi, 0});
       }
       if (c_hi < n) {
         GemmArgs g = gemm_args(n, n - c_hi, kb, W + c_lo, ldw, snap + c_hi, n, W + c_hi, ldw);
-        cta_gemm_epi<OP_N, OP_N, G3>(g, reinterpret_cast<cplx*>(smem_raw), EpiGJ{W, ldw, pinv, c_lo, c_hi, c_hi});
+        if constexpr (TC) cta_gemm_tc_epi<OP_N, OP_N>(g, smem_raw, EpiGJ{W, ldw, pinv, c_lo, c_hi, c_hi});
+        else cta_gemm_epi<OP_N, OP_N, G3>(g, reinterpret_cast<cplx*>(smem_raw), EpiGJ{W, ldw, pinv, c_lo, c_hi, c_hi});
       }
       pc->mark(PH_INV_UPDATE);
     }
@@ -335,12 +354,13 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
   return flag;
 }
 
-// G3: complex products of the rank updates (Gauss/3M or conventional 4M).
-template <bool G3 = true>
+// G3: complex products of the rank updates (Gauss/3M or conventional 4M);
+// TC: outer update on the tensor-core 3xTF32 GEMM.
+template <bool G3 = true, bool TC = false>
 NEGF_DEV int cta_inverse(cplx* W, int64_t ldw, int n, cplx* G, int64_t ldg, char* smem_raw, PhaseClock* pc,
                          cplx* snap) {
-  if (n <= 256) return cta_inverse_nb<32, 1, G3>(W, ldw, n, G, ldg, smem_raw, pc, snap);
-  return cta_inverse_nb<16, 2, G3>(W, ldw, n, G, ldg, smem_raw, pc, snap);
+  if (n <= 256) return cta_inverse_nb<32, 1, G3, TC>(W, ldw, n, G, ldg, smem_raw, pc, snap);
+  return cta_inverse_nb<16, 2, G3, TC>(W, ldw, n, G, ldg, smem_raw, pc, snap);
 }
 
 }  // namespace negf

@@ -83,7 +83,7 @@ enum Op : int { OP_N = 0, OP_C = 1 /* conjugate transpose */, OP_K = 2 /* conjug
 // charged to the phase that just ended.  Every mark follows a __syncthreads.
 enum Phase {
   PH_FORM = 0, PH_GEMM_FWD, PH_INV_STAGE, PH_INV_PANEL, PH_INV_UPDATE, PH_INV_GATHER,
-  PH_GEMM_BWD, PH_LESSER, PH_DOS, PH_TRANS, PH_OTHER, NPH
+  PH_GEMM_BWD, PH_LESSER, PH_DOS, PH_TRANS, PH_OTHER, PH_REFINE, NPH
 };
 struct PhaseClock {
   unsigned long long c[NPH];

@@ -6,7 +6,11 @@
 // and the T(E) / per-orbital DOS reductions -- keeping its intermediates in a
 // private scratch slot.  All contractions go through the CTA tile GEMM and the
 // blocked Gauss-Jordan inverse on FP64 tensor cores (cta_gemm.cuh,
-// cta_inverse.cuh).
+// cta_inverse.cuh); the mixed-precision variant (NEGF_MIXED) runs every block
+// product, including the inverse's outer update, on the tcgen05 3xTF32 GEMM
+// (cta_gemm_tc.cuh) and keeps pivoting, panels and storage in FP64.  Its
+// T(E) can be refined (NEGF_REFINE): one step of iterative refinement of the
+// column X = G_{:,N} with an FP64 residual, see rgf_item.
 //
 // Follows negf/recursive_green_cal.py (dpnegf):
 //   forward   g_0 = (-D_0)^-1,  g_q = (-D_q - L_{q-1} g_{q-1} U_{q-1})^-1     :88-94
@@ -34,7 +38,8 @@ struct SlotBufs {
   cplx* gslab;    // g_q storage when gr_left is not an output
   cplx* ginslab;  // lesser gin_q storage when gin_left is not an output
   cplx* grdslab;  // adjoint: G_qq of every block (when grd is not an output)
-  cplx* colslab;  // adjoint: G_qN of every block (when gr_lc is not an output)
+  cplx* colslab;  // adjoint / refinement: G_qN of every block (when gr_lc is not an output)
+  cplx* yslab;    // refinement: forward-substituted residual y_q of every block
   cplx *W, *T1, *Lz, *Uz, *gU, *Gd, *Gl, *Gu, *Gt0, *Gt1, *tA, *tB, *tC, *tD;
   cplx *Nd, *Nl, *Nu, *tE;  // lesser work
 };
@@ -44,10 +49,13 @@ __host__ __device__ inline size_t rgf_slot_elems(const NegfRgfProblem& p) {
   size_t e = RGF_NBUF * mn2;
   if (!(p.flags & NEGF_OUT_GR_LEFT)) e += (size_t)p.max_g_slab;
   if (p.flags & NEGF_LESSER) e += (size_t)p.max_g_slab;
-  if (p.flags & NEGF_ADJOINT) e += (size_t)p.max_g_slab + (size_t)p.col_slab;
+  if (p.flags & NEGF_ADJOINT) e += (size_t)p.max_g_slab;
+  if (p.flags & (NEGF_ADJOINT | NEGF_REFINE)) e += (size_t)p.col_slab;
+  if (p.flags & NEGF_REFINE) e += (size_t)p.col_slab;
   return (e + 15) & ~(size_t)15;  // keep slots 256-byte aligned
 }
 constexpr size_t RGF_SCRATCH_HEADER = 256;  // work-queue counter
+constexpr double REFINE_TOL = 1e-10;        // relative correction of G_1N that ends the refinement
 
 NEGF_DEV SlotBufs slot_bufs(const NegfRgfProblem& p, int slot) {
   cplx* base = reinterpret_cast<cplx*>(reinterpret_cast<char*>(p.scratch) + RGF_SCRATCH_HEADER) +
@@ -62,12 +70,12 @@ NEGF_DEV SlotBufs slot_bufs(const NegfRgfProblem& p, int slot) {
   s.ginslab = nullptr;
   s.grdslab = nullptr;
   s.colslab = nullptr;
+  s.yslab = nullptr;
   if (!(p.flags & NEGF_OUT_GR_LEFT)) { s.gslab = b; b += p.max_g_slab; }
   if (p.flags & NEGF_LESSER) { s.ginslab = b; b += p.max_g_slab; }
-  if (p.flags & NEGF_ADJOINT) {
-    s.grdslab = b; b += p.max_g_slab;
-    s.colslab = b; b += p.col_slab;
-  }
+  if (p.flags & NEGF_ADJOINT) { s.grdslab = b; b += p.max_g_slab; }
+  if (p.flags & (NEGF_ADJOINT | NEGF_REFINE)) { s.colslab = b; b += p.col_slab; }
+  if (p.flags & NEGF_REFINE) { s.yslab = b; b += p.col_slab; }
   return s;
 }
 
@@ -134,6 +142,19 @@ NEGF_DEV void form_gamma(cplx* out, const cplx* se, int ns, int r0, int c) {
   }
 }
 
+NEGF_DEV double cta_max(double v, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double s = red[0];
+  for (int w = 1; w < CTA_THREADS / 32; ++w) s = fmax(s, red[w]);
+  __syncthreads();
+  return s;
+}
+
 NEGF_DEV double cta_sum(double v, double* red) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -147,14 +168,23 @@ NEGF_DEV double cta_sum(double v, double* red) {
   return s;
 }
 
-template <int OPA, int OPB>
+// C = alpha op(A) op(B) (+ beta D) on the FP64 DMMA GEMM, or on the tcgen05
+// 3xTF32 GEMM when MX.
+template <int OPA, int OPB, bool MX>
 NEGF_DEV void gemm(cplx* smem, int M, int N, int K, const cplx* A, int64_t lda, const cplx* B, int64_t ldb,
                    cplx* C, int64_t ldc, cplx alpha = cmk(1.0, 0.0), const cplx* D = nullptr,
                    int64_t ldd = 0, cplx beta = cmk(1.0, 0.0)) {
   GemmArgs g = gemm_args(M, N, K, A, lda, B, ldb, C, ldc);
   g.alpha = alpha;
   if (D) { g.D = D; g.ldd = ldd; g.beta = beta; g.use_d = true; }
-  cta_gemm<OPA, OPB>(g, smem);
+  if constexpr (MX) cta_gemm_tc<OPA, OPB>(g, reinterpret_cast<char*>(smem));
+  else cta_gemm<OPA, OPB>(g, smem);
+}
+
+template <int OPA, int OPB, bool MX, class Epi>
+NEGF_DEV void gemm_epi(const GemmArgs& g, cplx* smem, const Epi& e) {
+  if constexpr (MX) cta_gemm_tc_epi<OPA, OPB>(g, reinterpret_cast<char*>(smem), e);
+  else cta_gemm_epi<OPA, OPB, true>(g, smem, e);
 }
 
 // Adjoint epilogue: W (rows of block q x cols of block p) contributes
@@ -187,6 +217,7 @@ struct EpiGrad {
   }
 };
 
+template <bool MX>
 NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBufs& sb, char* smem_raw,
                        double* red, PhaseClock& pc) {
   cplx* smem = reinterpret_cast<cplx*>(smem_raw);
@@ -228,29 +259,29 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
       form_shift(sb.Uz, hs, bp.hu, bp.su, z, np, nq, smem);  // U_{q-1}: n_{q-1} x n_q
       __syncthreads();
       pc.mark(PH_FORM);
-      gemm<OP_N, OP_N>(smem, nq, np, np, sb.Lz, np, gptr(q - 1), np, sb.T1, np);
-      gemm<OP_N, OP_N>(smem, nq, nq, np, sb.T1, np, sb.Uz, nq, sb.W, nq, MONE, sb.W, nq);
+      gemm<OP_N, OP_N, MX>(smem, nq, np, np, sb.Lz, np, gptr(q - 1), np, sb.T1, np);
+      gemm<OP_N, OP_N, MX>(smem, nq, nq, np, sb.T1, np, sb.Uz, nq, sb.W, nq, MONE, sb.W, nq);
       pc.mark(PH_GEMM_FWD);
     } else {
       __syncthreads();
       pc.mark(PH_FORM);
     }
-    bad |= cta_inverse(sb.W, nq, nq, gptr(q), nq, smem_raw, &pc, sb.tE);  // tE: pivot-row snapshot
+    bad |= cta_inverse<true, MX>(sb.W, nq, nq, gptr(q), nq, smem_raw, &pc, sb.tE);  // tE: pivot-row snapshot
     if (lesser) {
       // gin_q = g_q (s_q + L gin_{q-1} U) g_q^H
       const cplx* s = sinptr(q);
       if (q > 0) {
         const int np = blk[q - 1].n;
-        gemm<OP_N, OP_N>(smem, nq, np, np, sb.Lz, np, ginptr(q - 1), np, sb.T1, np);
-        if (s) gemm<OP_N, OP_N>(smem, nq, nq, np, sb.T1, np, sb.Uz, nq, sb.tA, nq, ONE, s, nq);
-        else gemm<OP_N, OP_N>(smem, nq, nq, np, sb.T1, np, sb.Uz, nq, sb.tA, nq);
+        gemm<OP_N, OP_N, MX>(smem, nq, np, np, sb.Lz, np, ginptr(q - 1), np, sb.T1, np);
+        if (s) gemm<OP_N, OP_N, MX>(smem, nq, nq, np, sb.T1, np, sb.Uz, nq, sb.tA, nq, ONE, s, nq);
+        else gemm<OP_N, OP_N, MX>(smem, nq, nq, np, sb.T1, np, sb.Uz, nq, sb.tA, nq);
       } else {
         if (s) copy_mat(sb.tA, s, nq, nq, smem);
         else for (int e = threadIdx.x; e < nq * nq; e += CTA_THREADS) sb.tA[e] = cmk(0.0, 0.0);
         __syncthreads();
       }
-      gemm<OP_N, OP_N>(smem, nq, nq, nq, gptr(q), nq, sb.tA, nq, sb.tB, nq);
-      gemm<OP_N, OP_C>(smem, nq, nq, nq, sb.tB, nq, gptr(q), nq, ginptr(q), nq);
+      gemm<OP_N, OP_N, MX>(smem, nq, nq, nq, gptr(q), nq, sb.tA, nq, sb.tB, nq);
+      gemm<OP_N, OP_C, MX>(smem, nq, nq, nq, sb.tB, nq, gptr(q), nq, ginptr(q), nq);
       pc.mark(PH_LESSER);
     }
   }
@@ -264,7 +295,7 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
   const int crA = seR ? min(nN, it.nse_r) : 0;
   // diag(G_qN Gamma_R G_qN^H) of block q from gt = G_qN (nq x nN); Gamma_R corner in sb.Nu
   auto spectral_diag = [&](double* dst, const cplx* gtq, int nq) {
-    gemm<OP_N, OP_N>(smem, nq, crA, crA, gtq + (nN - crA), nN, sb.Nu, crA, sb.W, crA);
+    gemm<OP_N, OP_N, MX>(smem, nq, crA, crA, gtq + (nN - crA), nN, sb.Nu, crA, sb.W, crA);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int i = warp; i < nq; i += CTA_THREADS / 32) {
       double acc = 0.0;
@@ -332,15 +363,15 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
     cplx* grl = (fl & NEGF_OUT_GRL) ? out + b.o_grl + row * szu : sb.Gl;
     cplx* gru = (fl & NEGF_OUT_GRU) ? out + b.o_gru + row * szu : sb.Gu;
     cplx* grd = (fl & NEGF_OUT_GRD) ? out + b.o_grd + row * sq(q) : (adj ? sb.grdslab + b.g : sb.Gd);
-    gemm<OP_N, OP_N>(smem, nq, nn, nq, g, nq, sb.Uz, nn, sb.gU, nn);         // gU = g U
-    gemm<OP_N, OP_N>(smem, nn, nq, nn, Gnext, nn, sb.Lz, nq, sb.T1, nq);     // G_{q+1,q+1} L
-    gemm<OP_N, OP_N>(smem, nn, nq, nq, sb.T1, nq, g, nq, grl, nq);           // grl
-    gemm<OP_N, OP_N>(smem, nq, nn, nn, sb.gU, nn, Gnext, nn, gru, nn);       // gru
-    gemm<OP_N, OP_N>(smem, nq, nq, nn, sb.gU, nn, grl, nq, grd, nq, ONE, g, nq);  // grd
+    gemm<OP_N, OP_N, MX>(smem, nq, nn, nq, g, nq, sb.Uz, nn, sb.gU, nn);         // gU = g U
+    gemm<OP_N, OP_N, MX>(smem, nn, nq, nn, Gnext, nn, sb.Lz, nq, sb.T1, nq);     // G_{q+1,q+1} L
+    gemm<OP_N, OP_N, MX>(smem, nn, nq, nq, sb.T1, nq, g, nq, grl, nq);           // grl
+    gemm<OP_N, OP_N, MX>(smem, nq, nn, nn, sb.gU, nn, Gnext, nn, gru, nn);       // gru
+    gemm<OP_N, OP_N, MX>(smem, nq, nq, nn, sb.gU, nn, grl, nq, grd, nq, ONE, g, nq);  // grd
     if (need_gt) {
       cplx* gtn = (fl & NEGF_OUT_GR_LC) ? out + b.o_grlc + row * (int64_t)nq * nN
-                                          : (adj ? sb.colslab + b.gc : (tog ? sb.Gt1 : sb.Gt0));
-      gemm<OP_N, OP_N>(smem, nq, nN, nn, sb.gU, nn, gt, nN, gtn, nN);
+                                          : (sb.colslab ? sb.colslab + b.gc : (tog ? sb.Gt1 : sb.Gt0));
+      gemm<OP_N, OP_N, MX>(smem, nq, nN, nn, sb.gU, nn, gt, nN, gtn, nN);
       gt = gtn;
       tog ^= 1;
     }
@@ -352,16 +383,16 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
       cplx* gnl = b.o_gnl >= 0 ? out + b.o_gnl + row * szu : sb.Nl;
       cplx* gnd = b.o_gnd >= 0 ? out + b.o_gnd + row * sq(q) : sb.Nd;
       // gLmH = L g^H  (n_{q+1} x n_q)
-      gemm<OP_N, OP_C>(smem, nn, nq, nq, sb.Lz, nq, g, nq, sb.tA, nq);
+      gemm<OP_N, OP_C, MX>(smem, nn, nq, nq, sb.Lz, nq, g, nq, sb.tA, nq);
       // gnl = G_{q+1,q+1} L gin + gnd_{q+1} gLmH ; sb.T1 still holds G_{q+1,q+1} L
-      gemm<OP_N, OP_N>(smem, nn, nq, nn, Nnext, nn, sb.tA, nq, sb.tB, nq);
-      gemm<OP_N, OP_N>(smem, nn, nq, nq, sb.T1, nq, gin, nq, gnl, nq, ONE, sb.tB, nq);
+      gemm<OP_N, OP_N, MX>(smem, nn, nq, nn, Nnext, nn, sb.tA, nq, sb.tB, nq);
+      gemm<OP_N, OP_N, MX>(smem, nn, nq, nq, sb.T1, nq, gin, nq, gnl, nq, ONE, sb.tB, nq);
       // gnd = gin + (g U) gnd_{q+1} gLmH + gin U gru^H + gru L gin
-      gemm<OP_N, OP_N>(smem, nq, nq, nn, sb.gU, nn, sb.tB, nq, sb.tC, nq, ONE, gin, nq);
-      gemm<OP_N, OP_N>(smem, nq, nn, nq, gin, nq, sb.Uz, nn, sb.tD, nn);
-      gemm<OP_N, OP_C>(smem, nq, nq, nn, sb.tD, nn, gru, nn, sb.tC, nq, ONE, sb.tC, nq);
-      gemm<OP_N, OP_N>(smem, nq, nq, nn, gru, nn, sb.Lz, nq, sb.tE, nq);
-      gemm<OP_N, OP_N>(smem, nq, nq, nq, sb.tE, nq, gin, nq, gnd, nq, ONE, sb.tC, nq);
+      gemm<OP_N, OP_N, MX>(smem, nq, nq, nn, sb.gU, nn, sb.tB, nq, sb.tC, nq, ONE, gin, nq);
+      gemm<OP_N, OP_N, MX>(smem, nq, nn, nq, gin, nq, sb.Uz, nn, sb.tD, nn);
+      gemm<OP_N, OP_C, MX>(smem, nq, nq, nn, sb.tD, nn, gru, nn, sb.tC, nq, ONE, sb.tC, nq);
+      gemm<OP_N, OP_N, MX>(smem, nq, nq, nn, gru, nn, sb.Lz, nq, sb.tE, nq);
+      gemm<OP_N, OP_N, MX>(smem, nq, nq, nq, sb.tE, nq, gin, nq, gnd, nq, ONE, sb.tC, nq);
       if (b.o_gnu >= 0) {
         cplx* gnu = out + b.o_gnu + row * szu;
         for (int e = threadIdx.x; e < nq * nn; e += CTA_THREADS) {
@@ -397,6 +428,83 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
   if (fl & NEGF_DOS) dos_total = 2.0 * cta_sum(dsum, red);
   pc.mark(PH_DOS);
 
+  // ------------------------------------------------------------ refinement
+  // Iterative refinement of the column X = G_{:,N} (X_q = G_qN), per step:
+  //   R_q  = delta_qN I - A_qq X_q + L_{q-1} X_{q-1} + U_q X_{q+1}   (FP64 tensor cores)
+  //   y_0 = R_0,  y_q = R_q + L_{q-1} g_{q-1} y_{q-1}
+  //   dX_N = g_N y_N,  dX_q = g_q (y_q + U_q dX_{q+1}),  X_q += dX_q  (sweep's product path)
+  // with A = zS - H - Sigma (A_{q,q-1} = -L_{q-1}, A_{q,q+1} = -U_q, the same
+  // sign convention as the forward sweep) and the stored left-connected g_q.
+  // Each step multiplies the error of X by the contraction of the approximate
+  // solve (about the relative error of the unrefined sweep, which grows with
+  // the number of blocks).  The item stops after refine_steps steps, or
+  // earlier once max|dX_0| <= REFINE_TOL max|X_0|.
+  if ((fl & NEGF_REFINE) && (fl & NEGF_TRANS) && seL && seR) {
+    const int steps = P.refine_steps > 0 ? P.refine_steps : 1;
+    auto colx = [&](int q) -> cplx* {
+      return (fl & NEGF_OUT_GR_LC) ? out + blk[q].o_grlc + row * (int64_t)blk[q].n * nN : sb.colslab + blk[q].gc;
+    };
+    if (!(fl & NEGF_OUT_GR_LC)) copy_mat(colx(K - 1), gptr(K - 1), nN, nN, smem);  // X_N apart from g_N
+    auto add_into = [&](cplx* x, const cplx* d, int64_t cnt) {
+      for (int64_t e = threadIdx.x; e < cnt; e += CTA_THREADS) x[e] = cadd(x[e], d[e]);
+      __syncthreads();
+    };
+    for (int step = 0; step < steps; ++step) {
+      for (int q = 0; q < K; ++q) {
+        const NegfBlock& b = blk[q];
+        const int nq = b.n;
+        cplx* yq = sb.yslab + b.gc;
+        form_a0(sb.W, hs, b, z, q == 0 ? seL : nullptr, it.nse_l, q == K - 1 ? seR : nullptr, it.nse_r, smem);
+        gemm<OP_N, OP_N, false>(smem, nq, nN, nq, sb.W, nq, colx(q), nN, yq, nN, MONE);  // -A_qq X_q
+        if (q == K - 1) {
+          for (int i = threadIdx.x; i < nN; i += CTA_THREADS) yq[(int64_t)i * nN + i].x += 1.0;
+          __syncthreads();
+        }
+        if (q > 0) {
+          const int np = blk[q - 1].n;
+          form_shift(sb.Lz, hs, blk[q - 1].hl, blk[q - 1].sl, z, nq, np, smem);
+          gemm<OP_N, OP_N, false>(smem, nq, nN, np, sb.Lz, np, colx(q - 1), nN, yq, nN, ONE, yq, nN);
+        }
+        if (q < K - 1) {
+          const int nn = b.n_next;
+          form_shift(sb.Uz, hs, b.hu, b.su, z, nq, nn, smem);
+          gemm<OP_N, OP_N, false>(smem, nq, nN, nn, sb.Uz, nn, colx(q + 1), nN, yq, nN, ONE, yq, nN);
+        }
+        if (q > 0) {
+          const int np = blk[q - 1].n;
+          gemm<OP_N, OP_N, MX>(smem, np, nN, np, gptr(q - 1), np, sb.yslab + blk[q - 1].gc, nN, sb.T1, nN);
+          gemm<OP_N, OP_N, MX>(smem, nq, nN, np, sb.Lz, np, sb.T1, nN, yq, nN, ONE, yq, nN);
+        }
+      }
+      cplx* dx = sb.Gt0;
+      cplx* dn = sb.Gt1;
+      gemm<OP_N, OP_N, MX>(smem, nN, nN, nN, gptr(K - 1), nN, sb.yslab + blk[K - 1].gc, nN, dx, nN);
+      add_into(colx(K - 1), dx, (int64_t)nN * nN);
+      for (int q = K - 2; q >= 0; --q) {
+        const NegfBlock& b = blk[q];
+        const int nq = b.n, nn = b.n_next;
+        form_shift(sb.Uz, hs, b.hu, b.su, z, nq, nn, smem);
+        gemm<OP_N, OP_N, MX>(smem, nq, nN, nn, sb.Uz, nn, dx, nN, sb.T1, nN, ONE, sb.yslab + b.gc, nN);
+        gemm<OP_N, OP_N, MX>(smem, nq, nN, nq, gptr(q), nq, sb.T1, nN, dn, nN);
+        add_into(colx(q), dn, (int64_t)nq * nN);
+        cplx* t = dx; dx = dn; dn = t;
+      }
+      if (step + 1 < steps) {  // dx holds dX_0
+        const cplx* x0 = colx(0);
+        double dmax = 0.0, xmax = 0.0;
+        for (int64_t e = threadIdx.x; e < (int64_t)blk[0].n * nN; e += CTA_THREADS) {
+          dmax = fmax(dmax, cabs1(dx[e]));
+          xmax = fmax(xmax, cabs1(x0[e]));
+        }
+        dmax = cta_max(dmax, red);
+        xmax = cta_max(xmax, red);
+        if (!(dmax > REFINE_TOL * xmax)) break;  // uniform: every thread sees the same maxima
+      }
+    }
+    gt = colx(0);
+    pc.mark(PH_REFINE);
+  }
+
   // ------------------------------------------------------------ T(E)
   double tval = 0.0;
   if ((fl & NEGF_TRANS) && seL && seR) {
@@ -406,8 +514,10 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
     form_gamma(sb.tA, seL, it.nse_l, 0, cl);
     form_gamma(sb.tB, seR, it.nse_r, it.nse_r - cr, cr);
     __syncthreads();
-    gemm<OP_N, OP_N>(smem, cl, cr, cl, sb.tA, cl, Gc, nN, sb.tC, cr);   // Gamma_L G
-    gemm<OP_N, OP_N>(smem, cl, cr, cr, sb.tC, cr, sb.tB, cr, sb.tD, cr);  // ... Gamma_R
+    // FP64 on both paths: per energy (not per block), and the mixed path's
+    // refined G_1N must not meet FP32-level products here
+    gemm<OP_N, OP_N, false>(smem, cl, cr, cl, sb.tA, cl, Gc, nN, sb.tC, cr);   // Gamma_L G
+    gemm<OP_N, OP_N, false>(smem, cl, cr, cr, sb.tC, cr, sb.tB, cr, sb.tD, cr);  // ... Gamma_R
     double part = 0.0;
     for (int e = threadIdx.x; e < cl * cr; e += CTA_THREADS) {
       int i = e / cr, l = e % cr;
@@ -435,13 +545,13 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
     cplx* gSl = gHl + u_slab;
     const cplx* Gc = gt + (nN - cr);  // G_1N[0:cl, nN-cr:], row stride nN
     cplx* Mc = sb.tE;                 // cr x cl
-    gemm<OP_N, OP_C>(smem, cr, cl, cr, sb.tB, cr, Gc, nN, sb.T1, cl);   // Gamma_R Gc^H
-    gemm<OP_N, OP_N>(smem, cr, cl, cl, sb.T1, cl, sb.tA, cl, Mc, cl);   // ... Gamma_L
+    gemm<OP_N, OP_C, MX>(smem, cr, cl, cr, sb.tB, cr, Gc, nN, sb.T1, cl);   // Gamma_R Gc^H
+    gemm<OP_N, OP_N, MX>(smem, cr, cl, cl, sb.T1, cl, sb.tA, cl, Mc, cl);   // ... Gamma_L
     // explicit Gamma terms: dT/dSigma_L = -2i K, K = Gc Gamma_R Gc^H; dT/dSigma_R = -2i Gc^H Gamma_L Gc
     cplx* gseL = reinterpret_cast<cplx*>(it.gse_l);
     cplx* gseR = reinterpret_cast<cplx*>(it.gse_r);
     if (gseL) {
-      gemm<OP_N, OP_N>(smem, cl, cl, cr, Gc, nN, sb.T1, cl, sb.Nd, cl);
+      gemm<OP_N, OP_N, MX>(smem, cl, cl, cr, Gc, nN, sb.T1, cl, sb.Nd, cl);
       const int ns = it.nse_l;
       for (int e = threadIdx.x; e < ns * ns; e += CTA_THREADS) {
         int i = e / ns, j = e % ns;
@@ -454,7 +564,7 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
       }
     }
     if (gseR) {
-      gemm<OP_C, OP_N>(smem, cr, cr, cl, Gc, nN, sb.tC, cr, sb.Nl, cr);  // Gc^H (Gamma_L Gc)
+      gemm<OP_C, OP_N, MX>(smem, cr, cr, cl, Gc, nN, sb.tC, cr, sb.Nl, cr);  // Gc^H (Gamma_L Gc)
       const int ns = it.nse_r, o = ns - cr;
       for (int e = threadIdx.x; e < ns * ns; e += CTA_THREADS) {
         int i = e / ns, j = e % ns;
@@ -484,35 +594,35 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
       int ldF;
       if (p == 0) { F = gpp(0); ldF = np; }
       else {
-        gemm<OP_N, OP_N>(smem, cl, np, np, Pc, np, gpp(p), np, sb.Lz, np);
+        gemm<OP_N, OP_N, MX>(smem, cl, np, np, Pc, np, gpp(p), np, sb.Lz, np);
         F = sb.Lz; ldF = np;
       }
-      gemm<OP_N, OP_N>(smem, cr, np, cl, Mc, cl, F, ldF, Ycur, np);       // Y_p = M_c F_p
+      gemm<OP_N, OP_N, MX>(smem, cr, np, cl, Mc, cl, F, ldF, Ycur, np);       // Y_p = M_c F_p
       const cplx* Rp = colp(p) + (nN - cr);
       {
         GemmArgs g = gemm_args(np, np, cr, Rp, nN, Ycur, np, nullptr, 0);
         EpiGrad e{gHd + blk[p].g, gSd + blk[p].g, np, c2, zc, p == 0 ? gseL : nullptr, cl, it.nse_l,
                   p == K - 1 ? gseR : nullptr, cr, it.nse_r, nN - cr};
-        cta_gemm_epi<OP_N, OP_N, true>(g, smem, e);                        // W_pp
+        gemm_epi<OP_N, OP_N, MX>(g, smem, e);                        // W_pp
       }
       if (p > 0) {  // W_{p-1,p} -> d/d(hl_{p-1}, sl_{p-1})  [n_p x n_{p-1}]
         const int nm = blk[p - 1].n;
         GemmArgs g = gemm_args(nm, np, cr, colp(p - 1) + (nN - cr), nN, Ycur, np, nullptr, 0);
         EpiGrad e{gHl + blk[p - 1].gu, gSl + blk[p - 1].gu, nm, c2, zc, nullptr, 0, 0, nullptr, 0, 0, 0};
-        cta_gemm_epi<OP_N, OP_N, true>(g, smem, e);
+        gemm_epi<OP_N, OP_N, MX>(g, smem, e);
       }
       if (p < K - 1) {
         const int nn = blk[p].n_next;
         {  // W_{p+1,p} -> d/d(hu_p, su_p)  [n_p x n_{p+1}]
           GemmArgs g = gemm_args(nn, np, cr, colp(p + 1) + (nN - cr), nN, Ycur, np, nullptr, 0);
           EpiGrad e{gHu + blk[p].gu, gSu + blk[p].gu, nn, c2, zc, nullptr, 0, 0, nullptr, 0, 0, 0};
-          cta_gemm_epi<OP_N, OP_N, true>(g, smem, e);
+          gemm_epi<OP_N, OP_N, MX>(g, smem, e);
         }
         // P_{p+1} = P_p g_p U_p
         form_shift(sb.Uz, hs, blk[p].hu, blk[p].su, z, np, nn, smem);
-        gemm<OP_N, OP_N>(smem, np, nn, np, gptr(p), np, sb.Uz, nn, sb.gU, nn);
+        gemm<OP_N, OP_N, MX>(smem, np, nn, np, gptr(p), np, sb.Uz, nn, sb.gU, nn);
         if (p == 0) copy_mat(Pn, sb.gU, cl, nn, smem);
-        else gemm<OP_N, OP_N>(smem, cl, nn, np, Pc, np, sb.gU, nn, Pn, nn);
+        else gemm<OP_N, OP_N, MX>(smem, cl, nn, np, Pc, np, sb.gU, nn, Pn, nn);
         cplx* t = Pc; Pc = Pn; Pn = t;
       }
     }
@@ -524,6 +634,7 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
     if (fl & NEGF_DOS) P.dos[it.out] = dos_total;
     int st = NEGF_OK;
     if (bad) st = NEGF_ERR_SINGULAR;
+    else if (MX && tc_err) st = NEGF_ERR_TIMEOUT;
     else if (!isfinite(tval) || !isfinite(dos_total)) st = NEGF_ERR_NONFINITE;
     P.status[it.out] = st;
   }
@@ -531,14 +642,16 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
   pc.mark(PH_TRANS);
 }
 
+template <bool MX>
 __global__ void __launch_bounds__(CTA_THREADS, 1) rgf_kernel(const NegfRgfProblem P) {
-  extern __shared__ __align__(16) char smem[];
+  extern __shared__ __align__(1024) char smem[];
   __shared__ int s_item;
   __shared__ double red[CTA_THREADS / 32];
   unsigned* queue = reinterpret_cast<unsigned*>(P.scratch);
   const SlotBufs sb = slot_bufs(P, blockIdx.x);
   PhaseClock pc;
   pc.start(P.phase_cycles != nullptr);
+  if constexpr (MX) tc_tmem_alloc();
   for (;;) {
     if (threadIdx.x == 0) s_item = (int)atomicAdd(queue, 1u);
     __syncthreads();
@@ -547,16 +660,17 @@ __global__ void __launch_bounds__(CTA_THREADS, 1) rgf_kernel(const NegfRgfProble
     pc.mark(PH_OTHER);
     if (idx >= P.n_items) break;
     const NegfItem it = P.items[idx];
-    rgf_item(P, it, sb, smem, red, pc);
+    rgf_item<MX>(P, it, sb, smem, red, pc);
   }
+  if constexpr (MX) tc_tmem_free();
   if (pc.on)
     for (int i = 0; i < NPH; ++i) P.phase_cycles[(size_t)blockIdx.x * NPH + i] = pc.c[i];
 }
 
 // Dynamic shared memory: the union of the GEMM ring, the inverse panel and the
 // streaming buffers (they are used one after another).
-size_t rgf_smem_bytes(int max_n) {
-  size_t a = GEMM_SMEM_BYTES, b = inv_smem_bytes_host(max_n), c = STREAM_SMEM_BYTES;
+size_t rgf_smem_bytes(int max_n, bool mixed) {
+  size_t a = mixed ? TC_SMEM_BYTES : GEMM_SMEM_BYTES, b = inv_smem_bytes_host(max_n, mixed), c = STREAM_SMEM_BYTES;
   size_t m = a > b ? a : b;
   return m > c ? m : c;
 }
@@ -586,17 +700,20 @@ int negf_rgf_run(const NegfRgfProblem* p, void* stream) {
   if ((p->flags & NEGF_ADJOINT) &&
       (!p->grad || p->grad_slab <= 0 || p->col_slab <= 0 || !(p->flags & NEGF_TRANS)))
     return NEGF_ERR_ARGUMENT;
+  if ((p->flags & NEGF_REFINE) && (p->col_slab <= 0 || !(p->flags & NEGF_TRANS))) return NEGF_ERR_ARGUMENT;
   const uint32_t blockouts = NEGF_OUT_GTRANS | NEGF_OUT_GR_LC | NEGF_OUT_GRD | NEGF_OUT_GRL | NEGF_OUT_GRU |
                              NEGF_OUT_GR_LEFT | NEGF_LESSER;
   if ((p->flags & blockouts) && !p->out) return NEGF_ERR_ARGUMENT;
   if ((p->flags & NEGF_LESSER) && !p->s_in) return NEGF_ERR_ARGUMENT;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const size_t smem = negf::rgf_smem_bytes(p->max_n);
-  if (cudaFuncSetAttribute(negf::rgf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+  const bool mixed = (p->flags & NEGF_MIXED) != 0;
+  const size_t smem = negf::rgf_smem_bytes(p->max_n, mixed);
+  auto kern = mixed ? negf::rgf_kernel<true> : negf::rgf_kernel<false>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return NEGF_ERR_CUDA;
   if (cudaMemsetAsync(p->scratch, 0, negf::RGF_SCRATCH_HEADER, s) != cudaSuccess) return NEGF_ERR_CUDA;
   const int grid = p->n_slots < p->n_items ? p->n_slots : p->n_items;
-  negf::rgf_kernel<<<grid, negf::CTA_THREADS, smem, s>>>(*p);
+  kern<<<grid, negf::CTA_THREADS, smem, s>>>(*p);
   return cudaGetLastError() == cudaSuccess ? NEGF_OK : NEGF_ERR_CUDA;
 }
 

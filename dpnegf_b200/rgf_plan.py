@@ -169,7 +169,8 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
         se_r: List[Optional[torch.Tensor]], eta=0.0, E_ref=0.0, outputs=("g_trans", "grd", "grl", "gru"),
         trans=False, orb_dos=False, dos=False, orb_g=False, orb_ar=False,
         s_in: Optional[List[List[Optional[torch.Tensor]]]] = None,
-        n_slots=None, check=True, stream=None, phase=False, events=None, adjoint_w=None):
+        n_slots=None, check=True, stream=None, phase=False, events=None, adjoint_w=None,
+        precision="fp64", refine=False, refine_steps=1):
     """Run the batched sweep.
 
     ``energies[d]`` is a 1-D tensor of B_d energies for device d; ``se_l[d]``
@@ -182,7 +183,13 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     ``adjoint_w`` ([B] weights of T(E), single device) switches the adjoint
     on: the result carries d(sum w T)/d(hd, hu, hl, sd, su, sl) and per-energy
     dT/dSigma_L, dT/dSigma_R weighted by w (torch's complex convention).
+    ``precision="mixed"`` runs every block product on the tcgen05 3xTF32 GEMM
+    (FP32-accurate products; pivoting, panels and storage stay FP64);
+    ``refine=True`` (with ``trans``) adds ``refine_steps`` FP64-residual
+    refinement steps of the column G_{:,N} that T(E) is read from.
     """
+    if precision not in ("fp64", "mixed"):
+        raise ValueError(f"precision must be 'fp64' or 'mixed', not {precision!r}")
     _lib.require_cuda()
     lib = _lib.load()
     dev = geom.device
@@ -217,6 +224,12 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
             raise ValueError("the adjoint runs on a single device")
         flags |= _lib.ADJOINT | _lib.TRANS
         trans = True
+    if precision == "mixed":
+        flags |= _lib.MIXED
+    if refine:
+        if not trans:
+            raise ValueError("refine improves T(E): it needs trans=True")
+        flags |= _lib.REFINE
 
     blocks = geom.blocks.copy()
     devs = geom.devs.copy()
@@ -351,6 +364,9 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     prob.status = status_t.data_ptr()
     prob.flags = flags
     prob.n_slots = n_slots
+    if refine or adjoint:
+        prob.col_slab = max(int(geom.col_slab), 1)
+    prob.refine_steps = int(refine_steps)
     need = lib.negf_rgf_scratch_bytes(ctypes.byref(prob))
     scratch = torch.empty(max(need, 256), dtype=torch.uint8, device=dev)
     prob.scratch = scratch.data_ptr()
@@ -362,7 +378,6 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
         grad_t = torch.zeros((n_slots, max(grad_slab, 1)), dtype=C128, device=dev)
         prob.grad = grad_t.data_ptr()
         prob.grad_slab = grad_slab
-        prob.col_slab = max(int(geom.col_slab), 1)
         need = lib.negf_rgf_scratch_bytes(ctypes.byref(prob))
         if need > scratch.numel():
             scratch = torch.empty(need, dtype=torch.uint8, device=dev)
@@ -399,6 +414,8 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
             if code == _lib.NEGF_ERR_SINGULAR:
                 raise torch.linalg.LinAlgError(
                     f"RGF: a left-connected block is singular (item {bad}); the matrix is not invertible")
+            if code == _lib.NEGF_ERR_TIMEOUT:
+                raise _lib.NegfError(f"RGF: a tensor-core completion wait expired (item {bad})")
             raise _lib.NegfError(f"RGF failed for item {bad} with status {code}")
     grads = None
     if adjoint:

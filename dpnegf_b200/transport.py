@@ -18,13 +18,18 @@ def transmission_dos(hd: Sequence[torch.Tensor], hu: Sequence[torch.Tensor], hl:
                      sd: Sequence[torch.Tensor], su: Sequence[torch.Tensor], sl: Sequence[torch.Tensor],
                      energy: torch.Tensor, left_se: torch.Tensor, right_se: torch.Tensor, eta: float = 0.0,
                      E_ref: float = 0.0, orbital_dos: bool = False,
-                     geometry: Optional[rgf_plan.Geometry] = None, device: str = "cuda", events=None):
+                     geometry: Optional[rgf_plan.Geometry] = None, device: str = "cuda", events=None,
+                     precision: str = "fp64", refine: bool = False, refine_steps: int = 1):
     """T(E) [B], DOS(E) [B] (spin factor 2) and optionally -Im diag(GS)/pi [B, n_orb].
 
     ``energy`` is a 1-D ``[B]`` tensor (real or complex); ``left_se`` /
     ``right_se`` are ``[B, n, n]`` lead self-energies embedded in the first /
     last block corners; ``eta`` is the device broadening (``eta_device``).
     Pass a prebuilt ``geometry`` to reuse the packed H/S arena across calls.
+    ``precision="mixed"`` computes the block products on the tcgen05 3xTF32
+    path (FP32-accurate); ``refine=True`` adds the FP64-residual refinement
+    of G_{:,N} that brings T(E) back to FP64-level accuracy (the DOS is not
+    refined).
     """
     out_dev = energy.device
     geom = geometry or rgf_plan.Geometry([rgf_plan.DeviceBlocks(hd, hu, hl, sd, su, sl)], device=device)
@@ -33,7 +38,8 @@ def transmission_dos(hd: Sequence[torch.Tensor], hu: Sequence[torch.Tensor], hl:
     seL = left_se.to(dev, non_blocking=True)
     seR = right_se.to(dev, non_blocking=True)
     res = rgf_plan.run(geom, [E], [seL], [seR], eta=eta, E_ref=E_ref, outputs=(), trans=True, dos=True,
-                       orb_dos=orbital_dos, events=events)
+                       orb_dos=orbital_dos, events=events, precision=precision, refine=refine,
+                       refine_steps=refine_steps)
     B = int(E.shape[0])
     T, D = res.trans, res.dos
     orb = res.orb_dos.view(B, -1) if orbital_dos else None

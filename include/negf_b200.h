@@ -36,6 +36,7 @@ extern "C" {
 #define NEGF_ERR_LS_RESIDUAL 3      /* residual >= 3e-5: surface_green.py:154 (ArithmeticError) */
 #define NEGF_ERR_SINGULAR 4         /* zero / non-finite pivot (torch.linalg.solve raises) */
 #define NEGF_ERR_NONFINITE 5        /* non-finite result */
+#define NEGF_ERR_TIMEOUT 6          /* a bounded tensor-core completion wait expired (NEGF_MIXED) */
 #define NEGF_ERR_ARGUMENT -1        /* malformed descriptor (call-level) */
 #define NEGF_ERR_UNSUPPORTED -2     /* block size above the compiled maximum (call-level) */
 #define NEGF_ERR_CUDA -3            /* CUDA launch / attribute error (call-level) */
@@ -57,10 +58,16 @@ extern "C" {
 #define NEGF_ORB_GDIAG (1u << 10)  /* diag(G_qq) per orbital (complex128)  -> orb_g[] */
 #define NEGF_ORB_AR (1u << 11)     /* diag(G_qN Gamma_R G_qN^H) per orbital -> orb_ar[] */
 #define NEGF_ADJOINT (1u << 12)    /* accumulate d(sum_items w_T T)/d(H, S) and dT/dSigma (single device) */
+#define NEGF_MIXED (1u << 13)      /* mixed precision: every block product on tcgen05 3xTF32 (FP32-accurate
+                                      products, FP32 accumulation); pivots, panels and storage stay FP64 */
+#define NEGF_REFINE (1u << 14)     /* with NEGF_TRANS: refine_steps iterative-refinement steps of the column
+                                      G_{:,N} before T(E) -- FP64 residual E_N - (zS - H - Sigma) G_{:,N} on
+                                      FP64 tensor cores, correction solved with the stored g_q (needs
+                                      col_slab); gr_lc outputs carry the refined column */
 
 /* Phase indices of NegfRgfProblem.phase_cycles (clock64 cycles per slot). */
-#define NEGF_PHASES 11 /* form, gemm_fwd, inv_stage, inv_panel, inv_update, inv_gather,
-                          gemm_bwd, lesser, dos, trans, other */
+#define NEGF_PHASES 12 /* form, gemm_fwd, inv_stage, inv_panel, inv_update, inv_gather,
+                          gemm_bwd, lesser, dos, trans, other, refine */
 
 /* One diagonal block q of a block-tridiagonal device. */
 typedef struct NegfBlock {
@@ -135,7 +142,10 @@ typedef struct NegfRgfProblem {
      Gradients follow torch's convention for complex inputs: dL/dRe + i dL/dIm. */
   double* grad;
   int64_t grad_slab;        /* complex elements per slot: 2 g_slab + 4 u_slab */
-  int64_t col_slab;         /* NEGF_ADJOINT: sum_q n_q n_N (last-column slab per slot) */
+  int64_t col_slab;         /* NEGF_ADJOINT / NEGF_REFINE: sum_q n_q n_N (last-column slab per slot) */
+  int32_t refine_steps;     /* NEGF_REFINE: at most this many refinement steps (<= 0 means 1); an item
+                               stops early once the correction to G_1N is below 1e-10 relative */
+  int32_t pad2;
 } NegfRgfProblem;
 
 /* ---- Lopez-Sancho lead decimation ------------------------------------ */

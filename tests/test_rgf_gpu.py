@@ -77,9 +77,10 @@ def _oracle_case(dims, B, seed, lesser=False, eta=1e-5):
 
 
 @pytest.mark.parametrize("dims,B", [([64] * 4, 3), ([70, 33, 128, 65], 2), ([256] * 3, 2),
-                                     ([300, 280], 1), ([17], 3), ([96, 96], 5)])
+                                     ([300, 280], 1), ([17], 3), ([96, 96], 5), ([240, 300], 1)])
 def test_rgf_matches_oracle_sizes(dims, B):
-    """Ragged tiles (n not a multiple of 64), the NB=16 inverse (n>256), K=1, K=2."""
+    """Ragged tiles (n not a multiple of 64), the NB=16 inverse (n>256), K=1, K=2, and a
+    device mixing both inverse layouts (the shared-memory size covers the larger)."""
     from dpnegf_b200.recursive_green_cal import recursive_gf
     dev, seL, seR, E, _ = _oracle_case(dims, B, seed=len(dims) * 7 + dims[0])
     ans = recursive_gf(E.cuda(), _cu(dev.hl), _cu(dev.hd), _cu(dev.hu), _cu(dev.sd), _cu(dev.su),

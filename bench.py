@@ -8,7 +8,11 @@ Gaussian sigma=0.01/sqrt(b), non-zero S couplings), 2048 energies in [-3,3] eV,
 eta=1e-5, complex128.  One step = one k-realisation (its own seeded device)
 over all 2048 energies: the full RGF sweep with T(E) and DOS reduced in the
 same launch.  Each rank handles its own k-realisations (weak scaling, no
-data-path collective).
+data-path collective).  The headline value is the plain FP64 sweep; the line
+also carries the mixed-precision sweep (tcgen05 3xTF32 products), its
+FP64-residual refined form with the T(E) error against the FP64 run, and the
+forward+adjoint throughput of both (``mixed`` and ``adjoint`` objects; one
+warm-up and one timed step each, rank 0 only).
 
 Prints one JSON line (rank 0).  ``--impl reference`` times the CPU oracle
 (numpy restatement of the reference recursive_gf + T/DOS) on the host cores
@@ -44,6 +48,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--phases", action="store_true", help="report per-phase SM-cycle shares")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision and adjoint legs")
+    ap.add_argument("--refine-steps", type=int, default=3)
     return ap.parse_args()
 
 
@@ -120,6 +126,29 @@ def measured_fp64_peak(torch):
         e1.record()
         torch.cuda.synchronize()
         best = min(best, e0.elapsed_time(e1))
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def measured_tf32_peak(torch):
+    """cuBLAS FP32 GEMM with TF32 tensor cores 8192^3, best of 5 -- the mixed path's denominator."""
+    n = 8192
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    a = torch.randn(n, n, dtype=torch.float32, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+    c = a @ b
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.mm(a, b, out=c)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    torch.backends.cuda.matmul.allow_tf32 = old
     del a, b, c
     torch.cuda.empty_cache()
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
@@ -271,10 +300,76 @@ def main():
 
     phases = None
     if args.phases:
-        r = step(args.warmup, phase=True)
+        phases = {}
+        for prec in ("fp64", "mixed"):
+            r = rgf_plan.run(geoms[args.warmup], [Ed], [seL], [seR], eta=args.eta, outputs=(), trans=True,
+                             dos=True, check=False, phase=True, precision=prec)
+            torch.cuda.synchronize()
+            pc = r.phase_cycles.sum(0).double()
+            phases[prec] = {n: float(v) for n, v in zip(_lib.PHASES, (pc / pc.sum()).tolist()) if v > 0}
+
+    # mixed precision and adjoint legs (rank 0): same devices, 1 warm-up + 1 timed step each
+    mixed = adjoint = None
+    if rank == 0 and not args.no_mixed:
+        sref = args.warmup  # first timed device; its FP64 T/DOS are the error reference
+        r64 = step(sref)
         torch.cuda.synchronize()
-        pc = r.phase_cycles.sum(0).double()
-        phases = {n: float(v) for n, v in zip(_lib.PHASES, (pc / pc.sum()).tolist())}
+        T64, D64 = r64.trans.cpu(), r64.dos.cpu()
+
+        def leg(fn):
+            fn(0)
+            torch.cuda.synchronize()
+            a, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            out = fn(sref)
+            b_.record()
+            torch.cuda.synchronize()
+            return out, a.elapsed_time(b_)
+
+        def mstep(s, **kw):
+            return rgf_plan.run(geoms[s], [Ed], [seL], [seR], eta=args.eta, outputs=(), trans=True, dos=True,
+                                check=False, precision="mixed", **kw)
+
+        rm, msm = leg(lambda s: mstep(s))
+        rr, msr = leg(lambda s: mstep(s, refine=True, refine_steps=args.refine_steps))
+        tf32 = measured_tf32_peak(torch)
+        v_m, v_r = B / (msm * 1e-3), B / (msr * 1e-3)
+        ach_m = flops_per_point(b, L) * v_m / 1e12
+        mixed = {
+            "value": v_m, "unit": UNIT, "speedup_vs_fp64": v_m / value,
+            "t_abs_err_max": float((rm.trans.cpu() - T64).abs().max()),
+            "dos_rel_err_max": float(((rm.dos.cpu() - D64).abs() / D64.abs()).max()),
+            "refined": {"value": v_r, "unit": UNIT, "speedup_vs_fp64": v_r / value,
+                        "refine_steps_max": args.refine_steps,
+                        "t_abs_err_max": float((rr.trans.cpu() - T64).abs().max())},
+            "roofline": {"bound": "tensor", "achieved": ach_m, "peak": tf32, "unit": "TFLOP/s",
+                         "frac": ach_m / tf32,
+                         "tensor_frac_executed": 3.0 * ach_m / tf32,
+                         "peak_source": "cuBLAS TF32 GEMM 8192^3 measured in this run (of measured)",
+                         "note": "algorithmic 72*b^3*L flop per point as for FP64; the 3xTF32 split "
+                                 "executes 3x that on the tensor cores"},
+            "precision": "complex products as 3xTF32 split on tcgen05.mma kind::tf32 (FP32 accumulation "
+                         "in TMEM); pivoting, panels and storage FP64; refined = FP64-residual steps on "
+                         "G_{:,N} (early stop at 1e-10 relative)",
+            "timing": f"1 warm-up + 1 timed step ({B} energies), CUDA events, rank 0"}
+        w = torch.ones(B, dtype=torch.float64)
+        adjoint = {}
+        for prec in ("fp64", "mixed"):
+            def fwd(s, prec=prec):
+                return rgf_plan.run(geoms[s], [Ed], [seL], [seR], eta=args.eta, outputs=(), trans=True,
+                                    check=False, precision=prec)
+
+            def adj(s, prec=prec):
+                return rgf_plan.run(geoms[s], [Ed], [seL], [seR], eta=args.eta, outputs=(), check=False,
+                                    adjoint_w=w, precision=prec)
+            _, tf = leg(fwd)
+            _, ta = leg(adj)
+            adjoint[prec] = {"value": B / ((tf + ta) * 1e-3), "unit": UNIT,
+                             "forward_value": B / (tf * 1e-3), "grad_over_forward": ta / tf}
+        adjoint["mixed_vs_fp64"] = adjoint["mixed"]["value"] / adjoint["fp64"]["value"]
+        adjoint["note"] = ("value = energy points/s of T(E) plus the full gradient d(sum T)/d(all H, S "
+                           "blocks, both self-energies); grad_over_forward = adjoint pass time / T-only "
+                           "forward time; 1 warm-up + 1 timed step each")
 
     # end-to-end through the public API: pinned host inputs, host outputs
     e2e = None
@@ -320,6 +415,9 @@ def main():
                 "gpu_launches": args.steps, "kernel_ms": kms}
         if phases:
             line["phases"] = phases
+        if mixed:
+            line["mixed"] = mixed
+            line["adjoint"] = adjoint
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

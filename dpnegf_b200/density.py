@@ -17,6 +17,9 @@ M_cut + 1 scalar round trips.
 ``integrate_orbitals`` is the block-tridiagonal generalisation: the
 per-orbital density over every block from the in-sweep reductions diag(G_qq)
 and diag(G_qN Gamma_R G_qN^H), without materialising Green's-function blocks.
+``uneven_batch`` does the same, plus T(E) in the bias window, for many devices
+of uneven block size and length: one Lopez-Sancho launch for every lead at
+every energy and one persistent RGF launch for every (device, energy) item.
 """
 import logging
 
@@ -139,3 +142,63 @@ class Ozaki(Density):
         else:
             n_neq = torch.zeros(n_orb, dtype=torch.float64, device=g.device)
         return n_eq, n_neq
+
+    def uneven_batch(self, devices, leads, kBT, mu_L, mu_D=0.0, vL=0.0, vR=0.0, fermi_L=None, fermi_R=None,
+                     eta_lead=1e-5, eta_device=0.0, E_ref=0.0, precision="fp64", refine=False, refine_steps=3,
+                     device="cuda"):
+        """Per-orbital density and T(E) of many BTD devices in one lead launch + one RGF launch.
+
+        ``devices`` are ``rgf_plan.DeviceBlocks``; ``leads[d] = (left, right)`` are
+        ``surface_green.LeadBlocks`` whose ``hDL`` couples the lead to the first /
+        last block.  Energies (relative to ``E_ref``): the far pole ``iR - mu_D``,
+        the Ozaki poles ``i pole kT + mu_L - mu_D`` and, when ``vL != vR``, the
+        ``n_gauss`` Gauss-Legendre points of ``[min V - 8kT, max V + 8kT]``; every
+        energy uses ``eta_lead`` for the leads and ``eta_device`` for the device.
+        Items are ordered largest first by the planner, so devices of very
+        different size balance over the persistent CTAs.  Returns one dict per
+        device: ``n_eq`` and ``n_neq`` [n_orb] (formulas of ``integrate_orbitals``),
+        and ``energy`` / ``trans`` on the real-axis points (empty without bias).
+        """
+        from . import rgf_plan
+        from .surface_green import LeadArena, self_energies
+        nd = len(devices)
+        if len(leads) != nd:
+            raise ValueError("one (left, right) lead pair per device")
+        P = len(self.poles)
+        zs = np.concatenate([[1j * self.R - mu_D], 1j * self.poles.numpy() * kBT + mu_L - mu_D]).astype(np.complex128)
+        bias = abs(vL - vR) > 1e-14
+        if bias:
+            xl, xu = min(vL, vR) - 8 * kBT, max(vL, vR) + 8 * kBT
+            xs, wlg = gauss_xw(xl=torch.scalar_tensor(xl, dtype=torch.float64),
+                               xu=torch.scalar_tensor(xu, dtype=torch.float64), n=self.n_gauss)
+            zs = np.concatenate([zs, xs.numpy().astype(np.complex128)])
+        nE = len(zs)
+        arena = LeadArena([ld for pair in leads for ld in pair], device=device)
+        idx = np.repeat(np.arange(2 * nd), nE)
+        ls = self_energies(arena, idx, np.tile(zs, 2 * nd), eta_lead, E_ref=E_ref)
+        se = [torch.stack(ls.sigma[i * nE:(i + 1) * nE]) for i in range(2 * nd)]
+        geom = rgf_plan.Geometry(list(devices), device=device)
+        E = torch.as_tensor(zs).to(geom.device)
+        res = rgf_plan.run(geom, [E] * nd, se[0::2], se[1::2], eta=eta_device, E_ref=E_ref, outputs=(),
+                           trans=True, orb_g=True, orb_ar=bias, precision=precision, refine=refine and bias,
+                           refine_steps=refine_steps)
+        r = self.residues.to(geom.device).reshape(-1, 1)
+        out, orb0 = [], 0
+        for d in range(nd):
+            n_orb = int(geom.devs[d]["n_orb"])
+            g = res.orb_g[orb0:orb0 + nE * n_orb].view(nE, n_orb)
+            n_eq = (1j * self.R * g[0] - ((-4j * kBT) * g[1:1 + P] * r).imag.sum(0)).real
+            rec = {"n_eq": n_eq, "energy": torch.zeros(0, dtype=torch.float64),
+                   "trans": torch.zeros(0, dtype=torch.float64, device=geom.device)}
+            if bias:
+                a = res.orb_ar[orb0:orb0 + nE * n_orb].view(nE, n_orb)[1 + P:]
+                e = xs.to(a.device)
+                df = (fermi_R(e + mu_D) - fermi_L(e + mu_D)).real.reshape(-1, 1)
+                rec["n_neq"] = (wlg.to(a.device).reshape(-1, 1) * a * df).sum(0)
+                rec["energy"] = xs
+                rec["trans"] = res.trans[d * nE + 1 + P:(d + 1) * nE]
+            else:
+                rec["n_neq"] = torch.zeros(n_orb, dtype=torch.float64, device=g.device)
+            out.append(rec)
+            orb0 += nE * n_orb
+        return out

@@ -139,6 +139,40 @@ class Geometry:
         return [int(x) for x in self.devs["n_orb"]]
 
 
+def check_status(status: torch.Tensor):
+    """Raise for the first failing item of a per-item status vector."""
+    st = status.cpu()
+    if (st != 0).any():
+        bad = int((st != 0).nonzero()[0, 0])
+        code = int(st[bad])
+        if code == _lib.NEGF_ERR_SINGULAR:
+            raise torch.linalg.LinAlgError(
+                f"RGF: a left-connected block is singular (item {bad}); the matrix is not invertible")
+        if code == _lib.NEGF_ERR_TIMEOUT:
+            raise _lib.NegfError(f"RGF: a tensor-core completion wait expired (item {bad})")
+        raise _lib.NegfError(f"RGF failed for item {bad} with status {code}")
+
+
+@dataclass
+class RgfPlan:
+    """A prepared sweep (``run(..., defer=True)``): descriptors, scratch and outputs stay allocated."""
+    prob: object
+    keep: list
+    n_items: int
+    result: "RgfResult"
+
+    def launch(self, stream=None):
+        """Enqueue the sweep on ``stream`` (default: the current stream).  No host synchronisation and
+        no allocation, so the call can be captured in a CUDA graph once the plan has run eagerly."""
+        if self.n_items:
+            _lib.check(_lib.load().negf_rgf_run(ctypes.byref(self.prob), _lib.stream_handle(stream)),
+                       "negf_rgf_run")
+
+    def check(self):
+        if self.n_items:
+            check_status(self.result.status)
+
+
 @dataclass
 class RgfResult:
     trans: Optional[torch.Tensor]    # [n_items] T(E), item order = device-major, energy-minor
@@ -170,7 +204,7 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
         trans=False, orb_dos=False, dos=False, orb_g=False, orb_ar=False,
         s_in: Optional[List[List[Optional[torch.Tensor]]]] = None,
         n_slots=None, check=True, stream=None, phase=False, events=None, adjoint_w=None,
-        precision="fp64", refine=False, refine_steps=1):
+        precision="fp64", refine=False, refine_steps=1, defer=False):
     """Run the batched sweep.
 
     ``energies[d]`` is a 1-D tensor of B_d energies for device d; ``se_l[d]``
@@ -187,6 +221,10 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     (FP32-accurate products; pivoting, panels and storage stay FP64);
     ``refine=True`` (with ``trans``) adds ``refine_steps`` FP64-residual
     refinement steps of the column G_{:,N} that T(E) is read from.
+    ``defer=True`` builds everything but launches nothing and returns an
+    ``RgfPlan``: its ``launch()`` re-runs the sweep on the same descriptors,
+    scratch and output tensors (a queue reset and one kernel, so it can be
+    captured in a CUDA graph) and its ``result`` views the outputs.
     """
     if precision not in ("fp64", "mixed"):
         raise ValueError(f"precision must be 'fp64' or 'mixed', not {precision!r}")
@@ -387,13 +425,19 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     if phase:
         phase_t = torch.zeros((n_slots, len(_lib.PHASES)), dtype=torch.int64, device=dev)
         prob.phase_cycles = phase_t.data_ptr()
-    # the staging tensors may be released on return: the caching allocator
-    # only hands their memory to work ordered after this launch on the stream
-    if events is not None:
-        events[0].record(stream)
-    _lib.check(lib.negf_rgf_run(ctypes.byref(prob), _lib.stream_handle(stream)), "negf_rgf_run")
-    if events is not None:
-        events[1].record(stream)
+    if defer:
+        if adjoint:
+            raise ValueError("the adjoint pass is not available as a deferred plan")
+        keep = [blocks_t, devs_t, items_t, sin_t, out_t, trans_t, orb_t, dos_t, orbg_t, orbar_t, status_t,
+                scratch, phase_t, geom.hs] + keep_alive
+    # otherwise the staging tensors may be released on return: the caching
+    # allocator only hands their memory to work ordered after this launch
+    if not defer:
+        if events is not None:
+            events[0].record(stream)
+        _lib.check(lib.negf_rgf_run(ctypes.byref(prob), _lib.stream_handle(stream)), "negf_rgf_run")
+        if events is not None:
+            events[1].record(stream)
 
     res_blocks = []
     for d in range(nd):
@@ -406,17 +450,14 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
             else:
                 dd[tag] = [out_t[off:off + B * s[0] * s[1]].view(B, *s) for off, s, B in v]
         res_blocks.append(dd)
+    if defer:
+        return RgfPlan(prob=prob, keep=keep, n_items=n_items, result=RgfResult(
+            trans=trans_t[:item_cursor] if trans else None, orb_dos=orb_t[:orb_cursor] if orb_dos else None,
+            dos=dos_t[:item_cursor] if dos else None, status=status_t[:item_cursor], blocks=res_blocks,
+            phase_cycles=phase_t, orb_g=orbg_t[:orb_cursor] if orb_g else None,
+            orb_ar=orbar_t[:orb_cursor] if orb_ar else None))
     if check and n_items:
-        st = status_t[:n_items].cpu()
-        if (st != 0).any():
-            bad = int((st != 0).nonzero()[0, 0])
-            code = int(st[bad])
-            if code == _lib.NEGF_ERR_SINGULAR:
-                raise torch.linalg.LinAlgError(
-                    f"RGF: a left-connected block is singular (item {bad}); the matrix is not invertible")
-            if code == _lib.NEGF_ERR_TIMEOUT:
-                raise _lib.NegfError(f"RGF: a tensor-core completion wait expired (item {bad})")
-            raise _lib.NegfError(f"RGF failed for item {bad} with status {code}")
+        check_status(status_t[:n_items])
     grads = None
     if adjoint:
         gsum = grad_t.sum(0)

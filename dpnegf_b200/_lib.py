@@ -106,7 +106,7 @@ class NegfRgfProblem(ctypes.Structure):
         ("grad_slab", ctypes.c_int64),
         ("col_slab", ctypes.c_int64),
         ("refine_steps", ctypes.c_int32),
-        ("pad2", ctypes.c_int32),
+        ("inv_ob", ctypes.c_int32),
     ]
 
 

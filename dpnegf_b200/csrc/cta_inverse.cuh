@@ -32,7 +32,8 @@
 
 namespace negf {
 
-constexpr int INV_OB = 128;  // outer block (columns) of the two-level Gauss-Jordan
+constexpr int INV_OB = 128;      // default outer block (columns) of the two-level Gauss-Jordan
+constexpr int INV_OB_MAX = 512;  // widest outer block (one block: no outer update for n <= 512)
 
 // Shared memory: panel, R tiles, pivot row and multiplier columns, then the
 // integer maps (piv, pinv, reductions).  With the tensor-core outer update
@@ -116,7 +117,7 @@ struct EpiGJ {
 // the outer update on the tcgen05 3xTF32 GEMM (FP32-accurate products).
 template <int NB, int RT, bool G3, bool TC>
 __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G, int64_t ldg, char* smem_raw,
-                                           PhaseClock* pc, cplx* snap) {
+                                           PhaseClock* pc, cplx* snap, int ob_max) {
   constexpr int PP = InvLayout<NB>::PP;
   constexpr int RP = InvLayout<NB>::RP;
   constexpr int NWARP = CTA_THREADS / 32;
@@ -161,7 +162,7 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
     return bi;
   };
 
-  const int ob = n <= INV_OB ? n : INV_OB;
+  const int ob = n <= ob_max ? n : ob_max;
   for (int c_lo = 0; c_lo < n; c_lo += ob) {
     const int c_hi = min(c_lo + ob, n);
     for (int p0 = c_lo; p0 < c_hi; p0 += NB) {
@@ -262,7 +263,7 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
         }
         cp_async_commit();
       };
-      int tiles[INV_OB / GT_N + 1];
+      int tiles[INV_OB_MAX / GT_N + 1];
       int ntile = 0;
       for (int c0 = c_lo; c0 < c_hi; c0 += GT_N) {
         const int c1 = min(c0 + GT_N, c_hi);
@@ -355,12 +356,15 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
 }
 
 // G3: complex products of the rank updates (Gauss/3M or conventional 4M);
-// TC: outer update on the tensor-core 3xTF32 GEMM.
+// TC: outer update on the tensor-core 3xTF32 GEMM.  ob: outer block width,
+// a multiple of 32 up to INV_OB_MAX (narrower blocks move work from the
+// panels' rank-NB updates to the outer GEMM; ob >= n leaves no outer update).
+// With ob < n the snapshot needs ob x n complex elements.
 template <bool G3 = true, bool TC = false>
 NEGF_DEV int cta_inverse(cplx* W, int64_t ldw, int n, cplx* G, int64_t ldg, char* smem_raw, PhaseClock* pc,
-                         cplx* snap) {
-  if (n <= 256) return cta_inverse_nb<32, 1, G3, TC>(W, ldw, n, G, ldg, smem_raw, pc, snap);
-  return cta_inverse_nb<16, 2, G3, TC>(W, ldw, n, G, ldg, smem_raw, pc, snap);
+                         cplx* snap, int ob = INV_OB) {
+  if (n <= 256) return cta_inverse_nb<32, 1, G3, TC>(W, ldw, n, G, ldg, smem_raw, pc, snap, ob);
+  return cta_inverse_nb<16, 2, G3, TC>(W, ldw, n, G, ldg, smem_raw, pc, snap, ob);
 }
 
 }  // namespace negf

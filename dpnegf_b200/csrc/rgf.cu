@@ -266,7 +266,8 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
       __syncthreads();
       pc.mark(PH_FORM);
     }
-    bad |= cta_inverse<true, MX>(sb.W, nq, nq, gptr(q), nq, smem_raw, &pc, sb.tE);  // tE: pivot-row snapshot
+    bad |= cta_inverse<true, MX>(sb.W, nq, nq, gptr(q), nq, smem_raw, &pc, sb.tE,  // tE: pivot-row snapshot
+                                 P.inv_ob > 0 ? P.inv_ob : INV_OB);
     if (lesser) {
       // gin_q = g_q (s_q + L gin_{q-1} U) g_q^H
       const cplx* s = sinptr(q);
@@ -701,6 +702,9 @@ int negf_rgf_run(const NegfRgfProblem* p, void* stream) {
       (!p->grad || p->grad_slab <= 0 || p->col_slab <= 0 || !(p->flags & NEGF_TRANS)))
     return NEGF_ERR_ARGUMENT;
   if ((p->flags & NEGF_REFINE) && (p->col_slab <= 0 || !(p->flags & NEGF_TRANS))) return NEGF_ERR_ARGUMENT;
+  if (p->inv_ob != 0 && p->inv_ob != 32 && p->inv_ob != 64 && p->inv_ob != 128 && p->inv_ob != 256 &&
+      p->inv_ob != 512)
+    return NEGF_ERR_ARGUMENT;
   const uint32_t blockouts = NEGF_OUT_GTRANS | NEGF_OUT_GR_LC | NEGF_OUT_GRD | NEGF_OUT_GRL | NEGF_OUT_GRU |
                              NEGF_OUT_GR_LEFT | NEGF_LESSER;
   if ((p->flags & blockouts) && !p->out) return NEGF_ERR_ARGUMENT;

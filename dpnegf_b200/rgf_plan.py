@@ -204,7 +204,7 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
         trans=False, orb_dos=False, dos=False, orb_g=False, orb_ar=False,
         s_in: Optional[List[List[Optional[torch.Tensor]]]] = None,
         n_slots=None, check=True, stream=None, phase=False, events=None, adjoint_w=None,
-        precision="fp64", refine=False, refine_steps=1, defer=False):
+        precision="fp64", refine=False, refine_steps=1, defer=False, inv_ob=None):
     """Run the batched sweep.
 
     ``energies[d]`` is a 1-D tensor of B_d energies for device d; ``se_l[d]``
@@ -221,6 +221,9 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     (FP32-accurate products; pivoting, panels and storage stay FP64);
     ``refine=True`` (with ``trans``) adds ``refine_steps`` FP64-residual
     refinement steps of the column G_{:,N} that T(E) is read from.
+    ``inv_ob`` is the inverse's outer block width (32..512); by default the
+    autotuned value for this GPU, block size and precision (``autotune.lookup``),
+    else 128.
     ``defer=True`` builds everything but launches nothing and returns an
     ``RgfPlan``: its ``launch()`` re-runs the sweep on the same descriptors,
     scratch and output tensors (a queue reset and one kernel, so it can be
@@ -405,6 +408,10 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     if refine or adjoint:
         prob.col_slab = max(int(geom.col_slab), 1)
     prob.refine_steps = int(refine_steps)
+    if inv_ob is None:
+        from . import autotune
+        inv_ob = autotune.lookup(geom.max_n, precision).get("inv_ob", 0)
+    prob.inv_ob = int(inv_ob)
     need = lib.negf_rgf_scratch_bytes(ctypes.byref(prob))
     scratch = torch.empty(max(need, 256), dtype=torch.uint8, device=dev)
     prob.scratch = scratch.data_ptr()

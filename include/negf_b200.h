@@ -145,7 +145,8 @@ typedef struct NegfRgfProblem {
   int64_t col_slab;         /* NEGF_ADJOINT / NEGF_REFINE: sum_q n_q n_N (last-column slab per slot) */
   int32_t refine_steps;     /* NEGF_REFINE: at most this many refinement steps (<= 0 means 1); an item
                                stops early once the correction to G_1N is below 1e-10 relative */
-  int32_t pad2;
+  int32_t inv_ob;           /* Gauss-Jordan outer block width: 32, 64, 128, 256 or 512 columns (0 = 128);
+                               results agree to rounding, the speed depends on block size and precision */
 } NegfRgfProblem;
 
 /* ---- Lopez-Sancho lead decimation ------------------------------------ */

@@ -126,3 +126,13 @@ def test_mixed_adjoint_close_to_fp64():
         err = np.abs(a - b).max() / np.abs(b).max()
         print(f"mixed adjoint gradient relative error {err:.2e}")
         assert err < FP32_RTOL
+
+
+@pytest.mark.parametrize("inv_ob", [32, 64, 128, 256])
+def test_mixed_outer_block_widths(inv_ob):
+    """The mixed sweep at every outer block width: refined T within 1e-6 of the oracle."""
+    dims = [200, 136, 200]
+    dev, seL, seR, E = _case(dims, 3, seed=51)
+    _, T, _ = _oracle(dev, seL, seR, E)
+    r = _run(dev, seL, seR, E, outputs=(), trans=True, precision="mixed", refine=True, inv_ob=inv_ob)
+    assert np.abs(r.trans.cpu().numpy() - T).max() < T_ATOL

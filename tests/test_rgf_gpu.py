@@ -172,3 +172,22 @@ def test_chain_transmission_is_one_in_band():
     inband = np.abs(E) < 1.9
     assert np.all(np.abs(T[inband] - 1.0) < 1e-4), T[inband]
     assert np.all(T[np.abs(E) > 2.1] < 1e-8)
+
+
+@pytest.mark.parametrize("inv_ob", [32, 64, 128, 256, 512])
+def test_inverse_outer_block_widths_agree(inv_ob):
+    """Every Gauss-Jordan outer block width (the autotuned knob) gives the oracle's
+    blocks to 1e-10, on sizes that use both panel layouts."""
+    from dpnegf_b200 import rgf_plan
+    dims = [200, 160, 300]
+    dev, seL, seR, E, _ = _oracle_case(dims, 2, seed=29)
+    geom = rgf_plan.Geometry([rgf_plan.DeviceBlocks(dev.hd, dev.hu, dev.hl, dev.sd, dev.su, dev.sl)])
+    res = rgf_plan.run(geom, [E.cuda()], [seL.cuda()], [seR.cuda()], eta=1e-5, outputs=("grd", "g_trans"),
+                       inv_ob=inv_ob)
+    ref = rgf_oracle.rgf(E.numpy(), [x.numpy() for x in dev.hl], [x.numpy() for x in dev.hd],
+                         [x.numpy() for x in dev.hu], [x.numpy() for x in dev.sd],
+                         [x.numpy() for x in dev.su], [x.numpy() for x in dev.sl],
+                         seL.numpy(), seR.numpy(), eta=1e-5)
+    for q, w in enumerate(ref["grd"]):
+        _assert_block_close(res.blocks[0]["grd"][q], w, f"grd[{q}] ob={inv_ob}")
+    _assert_block_close(res.blocks[0]["g_trans"], ref["g_trans"], f"g_trans ob={inv_ob}")

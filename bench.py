@@ -187,7 +187,8 @@ def cpu_baseline(args, seed, target_seconds=20.0):
     E = np.linspace(-3.0, 3.0, args.energies)[:: max(1, args.energies // nE)][:nE]
     seL, seR = cb._self_energies(args.b, len(E), seed)
     T, D, wall = cb.run_sample(args.b, args.L, seed, E, seL, seR, args.eta, procs)
-    return {"value": len(E) / wall, "unit": UNIT, "cores": procs, "kind": "port",
+    return {"value": len(E) / wall, "unit": UNIT, "cores": procs, "kind": "port", "seconds": wall,
+            "energies": len(E),
             "sample": f"{len(E)} energies of the b={args.b} L={args.L} workload (k-seed {seed}), "
                       f"numpy oracle RGF + T/DOS, {procs} spawn processes x 1 BLAS thread, {wall:.1f} s"}
 
@@ -196,18 +197,22 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    vals = []
+    vals, secs = [], []
     base = None
     for s in range(args.warmup + args.steps):
         base = cpu_baseline(args, seed=1000 + s)
         if s >= args.warmup:
             vals.append(base["value"])
+            secs.append(base["seconds"])
     v = statistics.median(vals) if vals else base["value"]
+    ms = 1e3 * (statistics.median(secs) if secs else base["seconds"])
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
             "config": {"workload": f"random Hermitian TB device b={args.b} L={args.L}, energies in [-3,3] eV, "
-                                   f"eta={args.eta}, T(E)+DOS", "b": args.b, "L": args.L},
+                                   f"eta={args.eta}, T(E)+DOS; each step a bounded sample of "
+                                   f"{base['energies']} energies on the host cores",
+                       "b": args.b, "L": args.L, "energies_per_step": base["energies"]},
             "cpu_baseline": dict(base, value=v),
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

@@ -183,7 +183,7 @@ def cpu_baseline(args, seed, target_seconds=20.0):
     import numpy as np
     from oracle import cpu_baseline as cb
     procs = cpu_procs()
-    nE = args.cpu_energies or procs
+    nE = args.cpu_energies or 8 * procs  # about 10-20 s of host work
     E = np.linspace(-3.0, 3.0, args.energies)[:: max(1, args.energies // nE)][:nE]
     seL, seR = cb._self_energies(args.b, len(E), seed)
     T, D, wall = cb.run_sample(args.b, args.L, seed, E, seL, seR, args.eta, procs)

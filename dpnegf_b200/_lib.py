@@ -41,13 +41,15 @@ ORB_AR = 1 << 11
 ADJOINT = 1 << 12
 MIXED = 1 << 13
 REFINE = 1 << 14
+GREATER = 1 << 15
 PHASES = ("form", "gemm_fwd", "inv_stage", "inv_panel", "inv_update", "inv_gather", "gemm_bwd", "lesser",
           "dos", "trans", "other", "refine")
 
 # numpy mirrors of the descriptor structs (packed exactly like the C structs)
 BLOCK_FIELDS = ["hd", "sd", "hu", "su", "hl", "sl", "sdT", "suT", "slT", "orb0", "g", "gc", "gu", "o_grd", "o_grl", "o_gru",
                 "o_grlc",
-                "o_grleft", "o_gnd", "o_gnl", "o_gnu", "o_ginleft", "s_in"]
+                "o_grleft", "o_gnd", "o_gnl", "o_gnu", "o_ginleft", "s_in", "o_gpd", "o_gpl", "o_gpu",
+                "o_gipleft", "s_out"]
 BLOCK_DTYPE = np.dtype([("n", "<i4"), ("n_next", "<i4")] + [(f, "<i8") for f in BLOCK_FIELDS])
 DEVICE_DTYPE = np.dtype([("n_blocks", "<i4"), ("blk0", "<i4"), ("n_orb", "<i4"), ("pad", "<i4"),
                          ("o_gtrans", "<i8"), ("g_slab", "<i8")])
@@ -107,6 +109,7 @@ class NegfRgfProblem(ctypes.Structure):
         ("col_slab", ctypes.c_int64),
         ("refine_steps", ctypes.c_int32),
         ("inv_ob", ctypes.c_int32),
+        ("s_out", ctypes.c_void_p),
     ]
 
 

@@ -21,6 +21,11 @@
 //             gnl_q = G_{q+1,q+1} L gin_q + gnd_{q+1} L g_q^H
 //             gnd_q = gin_q + g_q U gnd_{q+1} L g_q^H + gin_q U G_{q,q+1}^H
 //                     + G_{q,q+1} L gin_q;  gnu_q = gnl_q^H                      :121-140
+//   greater   gip_0 = g_0 s'_0 g_0^*;  gip_{q+1} = g_{q+1}(s'_{q+1} + L gip_q U^*) g_{q+1}^*
+//             gpl_q = G_{q+1,q+1} L gip_q + gpd_{q+1} L^* g_q^*
+//             gpd_q = gip_q + g_q U gpd_{q+1} L^* g_q^* + gip_q U^* G_{q+1,q}^*
+//                     + G_{q,q+1} L gip_q;  gpu_q = gpl_q^H                      :143-161
+//             (^* is the elementwise conjugate, exactly as the reference writes it)
 // with D = H + Sigma - zS, L = hl - z sl, U = hu - z su (:75-78), and the
 // reductions of negf/device_property.py: T = Re Tr[G_L G_1N G_R G_1N^H]
 // (:374-406) and -Im diag(G_qq S_qq + G_{q,q+1} S_{q+1,q} + G_{q,q-1} S_{q-1,q})/pi
@@ -40,6 +45,8 @@ struct SlotBufs {
   cplx* grdslab;  // adjoint: G_qq of every block (when grd is not an output)
   cplx* colslab;  // adjoint / refinement: G_qN of every block (when gr_lc is not an output)
   cplx* yslab;    // refinement: forward-substituted residual y_q of every block
+  cplx* gipslab;  // greater gip_q storage when gip_left is not an output
+  cplx* Pd;       // greater: gpd_{q+1} when gpd is not an output
   cplx *W, *T1, *Lz, *Uz, *gU, *Gd, *Gl, *Gu, *Gt0, *Gt1, *tA, *tB, *tC, *tD;
   cplx *Nd, *Nl, *Nu, *tE;  // lesser work
 };
@@ -52,6 +59,7 @@ __host__ __device__ inline size_t rgf_slot_elems(const NegfRgfProblem& p) {
   if (p.flags & NEGF_ADJOINT) e += (size_t)p.max_g_slab;
   if (p.flags & (NEGF_ADJOINT | NEGF_REFINE)) e += (size_t)p.col_slab;
   if (p.flags & NEGF_REFINE) e += (size_t)p.col_slab;
+  if (p.flags & NEGF_GREATER) e += (size_t)p.max_g_slab + mn2;
   return (e + 15) & ~(size_t)15;  // keep slots 256-byte aligned
 }
 constexpr size_t RGF_SCRATCH_HEADER = 256;  // work-queue counter
@@ -71,11 +79,17 @@ NEGF_DEV SlotBufs slot_bufs(const NegfRgfProblem& p, int slot) {
   s.grdslab = nullptr;
   s.colslab = nullptr;
   s.yslab = nullptr;
+  s.gipslab = nullptr;
+  s.Pd = nullptr;
   if (!(p.flags & NEGF_OUT_GR_LEFT)) { s.gslab = b; b += p.max_g_slab; }
   if (p.flags & NEGF_LESSER) { s.ginslab = b; b += p.max_g_slab; }
   if (p.flags & NEGF_ADJOINT) { s.grdslab = b; b += p.max_g_slab; }
   if (p.flags & (NEGF_ADJOINT | NEGF_REFINE)) { s.colslab = b; b += p.col_slab; }
   if (p.flags & NEGF_REFINE) { s.yslab = b; b += p.col_slab; }
+  if (p.flags & NEGF_GREATER) {
+    s.gipslab = b; b += p.max_g_slab;
+    s.Pd = b; b += mn2;
+  }
   return s;
 }
 
@@ -229,11 +243,13 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
   const cplx z = cmk(it.z_re, it.z_im);
   const cplx* hs = reinterpret_cast<const cplx*>(P.hs);
   const cplx* sin = reinterpret_cast<const cplx*>(P.s_in);
+  const cplx* sout = reinterpret_cast<const cplx*>(P.s_out);
   cplx* out = reinterpret_cast<cplx*>(P.out);
   const cplx* seL = reinterpret_cast<const cplx*>(it.se_l);
   const cplx* seR = reinterpret_cast<const cplx*>(it.se_r);
   const cplx ONE = cmk(1.0, 0.0), MONE = cmk(-1.0, 0.0);
   const bool lesser = (fl & NEGF_LESSER) != 0;
+  const bool greater = (fl & NEGF_GREATER) != 0;
   int bad = 0;
 
   auto sq = [&](int q) { return (int64_t)blk[q].n * blk[q].n; };
@@ -245,6 +261,12 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
   };
   auto sinptr = [&](int q) -> const cplx* {
     return blk[q].s_in >= 0 ? sin + blk[q].s_in + row * sq(q) : nullptr;
+  };
+  auto gipptr = [&](int q) -> cplx* {
+    return blk[q].o_gipleft >= 0 ? out + blk[q].o_gipleft + row * sq(q) : sb.gipslab + blk[q].g;
+  };
+  auto soutptr = [&](int q) -> const cplx* {
+    return blk[q].s_out >= 0 ? sout + blk[q].s_out + row * sq(q) : nullptr;
   };
 
   // ------------------------------------------------------------ forward sweep
@@ -283,6 +305,23 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
       }
       gemm<OP_N, OP_N, MX>(smem, nq, nq, nq, gptr(q), nq, sb.tA, nq, sb.tB, nq);
       gemm<OP_N, OP_C, MX>(smem, nq, nq, nq, sb.tB, nq, gptr(q), nq, ginptr(q), nq);
+      pc.mark(PH_LESSER);
+    }
+    if (greater) {
+      // gip_q = g_q (s'_q + L gip_{q-1} U^*) g_q^*   (elementwise conjugates)
+      const cplx* s = soutptr(q);
+      if (q > 0) {
+        const int np = blk[q - 1].n;
+        gemm<OP_N, OP_N, MX>(smem, nq, np, np, sb.Lz, np, gipptr(q - 1), np, sb.T1, np);
+        if (s) gemm<OP_N, OP_K, MX>(smem, nq, nq, np, sb.T1, np, sb.Uz, nq, sb.tA, nq, ONE, s, nq);
+        else gemm<OP_N, OP_K, MX>(smem, nq, nq, np, sb.T1, np, sb.Uz, nq, sb.tA, nq);
+      } else {
+        if (s) copy_mat(sb.tA, s, nq, nq, smem);
+        else for (int e = threadIdx.x; e < nq * nq; e += CTA_THREADS) sb.tA[e] = cmk(0.0, 0.0);
+        __syncthreads();
+      }
+      gemm<OP_N, OP_N, MX>(smem, nq, nq, nq, gptr(q), nq, sb.tA, nq, sb.tB, nq);
+      gemm<OP_N, OP_K, MX>(smem, nq, nq, nq, sb.tB, nq, gptr(q), nq, gipptr(q), nq);
       pc.mark(PH_LESSER);
     }
   }
@@ -336,6 +375,15 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
       cplx* d = out + blk[K - 1].o_gnd + row * sq(K - 1);
       copy_mat(d, ginptr(K - 1), nN, nN, smem);
       Nnext = d;
+    }
+  }
+  const cplx* Pnext = nullptr;  // gpd_{q+1}
+  if (greater) {
+    Pnext = gipptr(K - 1);
+    if (blk[K - 1].o_gpd >= 0) {
+      cplx* d = out + blk[K - 1].o_gpd + row * sq(K - 1);
+      copy_mat(d, gipptr(K - 1), nN, nN, smem);
+      Pnext = d;
     }
   }
   __syncthreads();
@@ -403,6 +451,32 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
       }
       __syncthreads();
       Nnext = gnd;
+      pc.mark(PH_LESSER);
+    }
+    if (greater) {
+      const cplx* gip = gipptr(q);
+      cplx* gpl = b.o_gpl >= 0 ? out + b.o_gpl + row * szu : sb.Nl;
+      cplx* gpd = b.o_gpd >= 0 ? out + b.o_gpd + row * sq(q) : sb.Pd;
+      // lcgc = L^* g^*  (n_{q+1} x n_q)
+      gemm<OP_K, OP_K, MX>(smem, nn, nq, nq, sb.Lz, nq, g, nq, sb.tA, nq);
+      // gpl = G_{q+1,q+1} L gip + gpd_{q+1} lcgc ; sb.T1 still holds G_{q+1,q+1} L
+      gemm<OP_N, OP_N, MX>(smem, nn, nq, nn, Pnext, nn, sb.tA, nq, sb.tB, nq);
+      gemm<OP_N, OP_N, MX>(smem, nn, nq, nq, sb.T1, nq, gip, nq, gpl, nq, ONE, sb.tB, nq);
+      // gpd = gip + (g U) gpd_{q+1} lcgc + gip U^* grl^* + gru L gip
+      gemm<OP_N, OP_N, MX>(smem, nq, nq, nn, sb.gU, nn, sb.tB, nq, sb.tC, nq, ONE, gip, nq);
+      gemm<OP_N, OP_K, MX>(smem, nq, nn, nq, gip, nq, sb.Uz, nn, sb.tD, nn);
+      gemm<OP_N, OP_K, MX>(smem, nq, nq, nn, sb.tD, nn, grl, nq, sb.tC, nq, ONE, sb.tC, nq);
+      gemm<OP_N, OP_N, MX>(smem, nq, nq, nn, gru, nn, sb.Lz, nq, sb.tE, nq);
+      gemm<OP_N, OP_N, MX>(smem, nq, nq, nq, sb.tE, nq, gip, nq, gpd, nq, ONE, sb.tC, nq);
+      if (b.o_gpu >= 0) {
+        cplx* gpu = out + b.o_gpu + row * szu;
+        for (int e = threadIdx.x; e < nq * nn; e += CTA_THREADS) {
+          int i = e / nn, j = e % nn;  // gpu[i][j] = conj(gpl[j][i])
+          gpu[e] = cconj(gpl[(int64_t)j * nq + i]);
+        }
+      }
+      __syncthreads();
+      Pnext = gpd;
       pc.mark(PH_LESSER);
     }
     if (want_dos) {
@@ -706,9 +780,10 @@ int negf_rgf_run(const NegfRgfProblem* p, void* stream) {
       p->inv_ob != 512)
     return NEGF_ERR_ARGUMENT;
   const uint32_t blockouts = NEGF_OUT_GTRANS | NEGF_OUT_GR_LC | NEGF_OUT_GRD | NEGF_OUT_GRL | NEGF_OUT_GRU |
-                             NEGF_OUT_GR_LEFT | NEGF_LESSER;
+                             NEGF_OUT_GR_LEFT | NEGF_LESSER | NEGF_GREATER;
   if ((p->flags & blockouts) && !p->out) return NEGF_ERR_ARGUMENT;
   if ((p->flags & NEGF_LESSER) && !p->s_in) return NEGF_ERR_ARGUMENT;
+  if ((p->flags & NEGF_GREATER) && !p->s_out) return NEGF_ERR_ARGUMENT;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const bool mixed = (p->flags & NEGF_MIXED) != 0;
   const size_t smem = negf::rgf_smem_bytes(p->max_n, mixed);

@@ -83,8 +83,10 @@ class DeviceProperty(object):
                            HS_inmem: bool = True, need_lesser: bool = False, need_greater: bool = False,
                            need_gr_lc: bool = False):
         """Green's functions (and fused T, DOS, LDOS) at ``energy`` (scalar or [B]) for ``kpoint``."""
-        if need_greater:
-            raise NotImplementedError("need_greater=True (G^> sweep) is not provided by dpnegf_b200")
+        # the reference passes s_out=None to recursive_gf here (device_property.py:283), whose greater
+        # branch then fails its list check (recursive_green_cal.py:67 / :268): same error
+        assert not need_greater, \
+            "Greater Green's function calculation requires s_out to be a list of coupling matrices"
         assert len(np.array(kpoint).reshape(-1)) == 3
         dev = self._compute_device()
         energy = torch.as_tensor(energy, dtype=torch.complex128, device=dev)

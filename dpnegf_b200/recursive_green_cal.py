@@ -36,15 +36,16 @@ def recursive_gf(energy, hl, hd, hu, sd, su, sl, left_se, right_se, seP=None, E_
     or 3-D ``[B, ...]``.  ``left_se``/``right_se`` are ``[B, n, n]`` (2-D for a
     scalar energy) and are added to the top-left / bottom-right corner of the
     first / last diagonal block.  ``s_in`` (list of K ``[B, n_q, n_q]``) feeds
-    the lesser sweep when ``need_lesser``.  Returns the 14-tuple
+    the lesser sweep when ``need_lesser``; ``s_out`` (same layout) feeds the
+    greater sweep when ``need_greater``.  Returns the 14-tuple
     ``(g_trans, gr_lc, grd, grl, gru, gr_left, gnd, gnl, gnu, gin_left,
     gpd, gpl, gpu, gip_left)``; the batch dim is squeezed for scalar callers
     (``left_se`` 2-D).
     """
-    if need_greater:
-        raise NotImplementedError("need_greater=True (G^> sweep) is not provided by dpnegf_b200")
     if need_lesser:
         assert isinstance(s_in, list), "Lesser Green's function calculation requires s_in to be a list of coupling matrices"
+    if need_greater:
+        assert isinstance(s_out, list), "Greater Green's function calculation requires s_out to be a list of coupling matrices"
 
     out_dev = hd[0].device if torch.is_tensor(hd[0]) else torch.device("cpu")
     dev = out_dev if out_dev.type == "cuda" else torch.device("cuda", torch.cuda.current_device()
@@ -88,13 +89,14 @@ def recursive_gf(energy, hl, hd, hu, sd, su, sl, left_se, right_se, seP=None, E_
         outputs.append("gr_lc")
     if keep_gr_left:
         outputs.append("gr_left")
-    sin = None
-    if need_lesser:
-        sin = []
+
+    def per_device(src):
+        """Per-device lists of per-block [B_d, n, n] inputs (None = zero block)."""
+        res = []
         for d in range(len(devices)):
             lst = []
             for q in range(K):
-                t = s_in[q]
+                t = src[q]
                 if not torch.is_tensor(t):
                     lst.append(None)
                     continue
@@ -103,10 +105,14 @@ def recursive_gf(energy, hl, hd, hu, sd, su, sl, left_se, right_se, seP=None, E_
                 elif per_energy:
                     t = t[d:d + 1]
                 lst.append(t)
-            sin.append(lst)
+            res.append(lst)
+        return res
+
+    sin = per_device(s_in) if need_lesser else None
+    sout = per_device(s_out) if need_greater else None
     res = rgf_plan.run(geom, energies, [se_for(left_se, d) for d in range(len(devices))],
                        [se_for(right_se, d) for d in range(len(devices))], eta=eta, E_ref=0.0,
-                       outputs=outputs, s_in=sin)
+                       outputs=outputs, s_in=sin, s_out=sout)
 
     def gather(tag):
         if tag not in res.blocks[0]:
@@ -117,7 +123,7 @@ def recursive_gf(energy, hl, hd, hu, sd, su, sl, left_se, right_se, seP=None, E_
             return torch.cat([r[tag] for r in res.blocks], 0)
         return [torch.cat([r[tag][q] for r in res.blocks], 0) for q in range(len(res.blocks[0][tag]))]
 
-    vals = {t: gather(t) for t in TAGS[:10]}
+    vals = {t: gather(t) for t in TAGS}
     ans = tuple(vals.get(t) for t in TAGS)
     if out_dev.type != "cuda":
         ans = _to(ans, out_dev)

@@ -100,7 +100,7 @@ class Geometry:
                 if q + 1 < K:
                     gu += n * dims[q + 1]
                 for f in ("o_grd", "o_grl", "o_gru", "o_grlc", "o_grleft", "o_gnd", "o_gnl", "o_gnu",
-                          "o_ginleft", "s_in"):
+                          "o_ginleft", "s_in", "o_gpd", "o_gpl", "o_gpu", "o_gipleft", "s_out"):
                     b[f] = -1
                 blocks.append(b)
                 g += n * n
@@ -196,6 +196,10 @@ _FAMILY = {  # output tag -> (flag, block field, shape fn (n_q, n_next, n_last))
     "gnl": (_lib.LESSER, "o_gnl", lambda n, nn, nl: (nn, n), True),
     "gnu": (_lib.LESSER, "o_gnu", lambda n, nn, nl: (n, nn), True),
     "gin_left": (_lib.LESSER, "o_ginleft", lambda n, nn, nl: (n, n), False),
+    "gpd": (_lib.GREATER, "o_gpd", lambda n, nn, nl: (n, n), False),
+    "gpl": (_lib.GREATER, "o_gpl", lambda n, nn, nl: (nn, n), True),
+    "gpu": (_lib.GREATER, "o_gpu", lambda n, nn, nl: (n, nn), True),
+    "gip_left": (_lib.GREATER, "o_gipleft", lambda n, nn, nl: (n, n), False),
 }
 
 
@@ -203,6 +207,7 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
         se_r: List[Optional[torch.Tensor]], eta=0.0, E_ref=0.0, outputs=("g_trans", "grd", "grl", "gru"),
         trans=False, orb_dos=False, dos=False, orb_g=False, orb_ar=False,
         s_in: Optional[List[List[Optional[torch.Tensor]]]] = None,
+        s_out: Optional[List[List[Optional[torch.Tensor]]]] = None,
         n_slots=None, check=True, stream=None, phase=False, events=None, adjoint_w=None,
         precision="fp64", refine=False, refine_steps=1, defer=False, inv_ob=None):
     """Run the batched sweep.
@@ -211,7 +216,8 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     / ``se_r[d]`` are ``[B_d, n, n]`` self-energies (or None).  ``outputs``
     names the block tensors to materialise (tags of recursive_gf's tuple);
     ``s_in[d]`` is the per-block list of ``[B_d, n_q, n_q]`` lesser inputs
-    (None entries are zero blocks) and switches the lesser sweep on.
+    (None entries are zero blocks) and switches the lesser sweep on; ``s_out``
+    (same layout) switches the greater sweep on (gpd, gpl, gpu, gip_left).
     ``events=(start, end)`` are CUDA events recorded on the launch stream
     immediately around the kernel (device time of the sweep alone).
     ``adjoint_w`` ([B] weights of T(E), single device) switches the adjoint
@@ -239,6 +245,9 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     lesser = s_in is not None
     if lesser:
         outputs |= {"gnd", "gnl", "gnu", "gin_left"}
+    greater = s_out is not None
+    if greater:
+        outputs |= {"gpd", "gpl", "gpu", "gip_left"}
     flags = 0
     for tag in outputs:
         if tag == "g_trans":
@@ -259,6 +268,8 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
         flags |= _lib.ORB_AR
     if lesser:
         flags |= _lib.LESSER
+    if greater:
+        flags |= _lib.GREATER
     adjoint = adjoint_w is not None
     if adjoint:
         if nd != 1:
@@ -278,6 +289,8 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     layout = []  # per device: tag -> list of (offset, shape, B)
     sin_pieces = []
     sin_cursor = 0
+    sout_pieces = []
+    sout_cursor = 0
     item_parts, cost_parts = [], []
     keep_alive = []
     orb_cursor = 0
@@ -290,7 +303,8 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
         B = int(E.shape[0])
         lay = {}
         nl = dims[-1]
-        for tag in ("grd", "grl", "gru", "gr_lc", "gr_left", "gnd", "gnl", "gnu", "gin_left"):
+        for tag in ("grd", "grl", "gru", "gr_lc", "gr_left", "gnd", "gnl", "gnu", "gin_left",
+                    "gpd", "gpl", "gpu", "gip_left"):
             if tag not in outputs:
                 continue
             _, field, shp, offd = _FAMILY[tag]
@@ -339,6 +353,17 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
                 blocks[b0 + q]["s_in"] = sin_cursor
                 sin_pieces.append(t.reshape(-1))
                 sin_cursor += B * dims[q] * dims[q]
+        if greater:
+            for q in range(K):
+                t = s_out[d][q]
+                if t is None:
+                    continue
+                t = t.to(device=dev, dtype=C128)
+                if t.ndim == 2:
+                    t = t.unsqueeze(0).expand(B, -1, -1)
+                blocks[b0 + q]["s_out"] = sout_cursor
+                sout_pieces.append(t.reshape(-1))
+                sout_cursor += B * dims[q] * dims[q]
         z = (E.to(torch.complex128).cpu().numpy().reshape(-1) + complex(E_ref)) + 1j * float(eta)
         n_orb = int(devs[d]["n_orb"])
         rows = np.arange(B, dtype=np.int64)
@@ -378,6 +403,7 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     devs_t = u8(devs)
     items_t = u8(item_arr) if n_items else torch.zeros(1, dtype=torch.uint8, device=dev)
     sin_t = torch.cat(sin_pieces) if sin_pieces else torch.zeros(1, dtype=C128, device=dev)
+    sout_t = torch.cat(sout_pieces) if sout_pieces else torch.zeros(1, dtype=C128, device=dev)
     out_t = torch.empty(max(out_cursor, 1), dtype=C128, device=dev)
     trans_t = torch.empty(max(item_cursor, 1), dtype=torch.float64, device=dev) if trans else None
     orb_t = torch.empty(max(orb_cursor, 1), dtype=torch.float64, device=dev) if orb_dos else None
@@ -396,6 +422,7 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     prob.max_g_slab = geom.max_g_slab
     prob.hs = geom.hs.data_ptr()
     prob.s_in = sin_t.data_ptr()
+    prob.s_out = sout_t.data_ptr()
     prob.out = out_t.data_ptr()
     prob.trans = trans_t.data_ptr() if trans else None
     prob.orb_dos = orb_t.data_ptr() if orb_dos else None
@@ -435,7 +462,7 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     if defer:
         if adjoint:
             raise ValueError("the adjoint pass is not available as a deferred plan")
-        keep = [blocks_t, devs_t, items_t, sin_t, out_t, trans_t, orb_t, dos_t, orbg_t, orbar_t, status_t,
+        keep = [blocks_t, devs_t, items_t, sin_t, sout_t, out_t, trans_t, orb_t, dos_t, orbg_t, orbar_t, status_t,
                 scratch, phase_t, geom.hs] + keep_alive
     # otherwise the staging tensors may be released on return: the caching
     # allocator only hands their memory to work ordered after this launch

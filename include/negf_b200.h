@@ -64,6 +64,8 @@ extern "C" {
                                       G_{:,N} before T(E) -- FP64 residual E_N - (zS - H - Sigma) G_{:,N} on
                                       FP64 tensor cores, correction solved with the stored g_q (needs
                                       col_slab); gr_lc outputs carry the refined column */
+#define NEGF_GREATER (1u << 15)    /* greater sweep from s_out: gip_left, gpd, gpl, gpu
+                                      (recursive_green_cal.py:143-161, :267-289) */
 
 /* Phase indices of NegfRgfProblem.phase_cycles (clock64 cycles per slot). */
 #define NEGF_PHASES 12 /* form, gemm_fwd, inv_stage, inv_panel, inv_update, inv_gather,
@@ -87,6 +89,8 @@ typedef struct NegfBlock {
   int64_t o_grd, o_grl, o_gru, o_grlc, o_grleft;
   int64_t o_gnd, o_gnl, o_gnu, o_ginleft;
   int64_t s_in; /* lesser input Sigma^in_q for batch row 0 in s_in; -1 = zero */
+  int64_t o_gpd, o_gpl, o_gpu, o_gipleft; /* NEGF_GREATER block outputs (same row rule); -1 = not produced */
+  int64_t s_out; /* greater input Sigma^out_q for batch row 0 in s_out; -1 = zero */
 } NegfBlock;
 
 /* One device (k-point / realisation): a run of n_blocks NegfBlock entries. */
@@ -147,6 +151,7 @@ typedef struct NegfRgfProblem {
                                stops early once the correction to G_1N is below 1e-10 relative */
   int32_t inv_ob;           /* Gauss-Jordan outer block width: 32, 64, 128, 256 or 512 columns (0 = 128);
                                results agree to rounding, the speed depends on block size and precision */
+  const double* s_out;      /* complex128 arena of Sigma^out blocks (NEGF_GREATER) */
 } NegfRgfProblem;
 
 /* ---- Lopez-Sancho lead decimation ------------------------------------ */
@@ -208,7 +213,7 @@ size_t negf_rgf_scratch_bytes(const NegfRgfProblem* p);
  * recursive_gf_cal (negf/recursive_green_cal.py:4-296): forward left-connected
  * g_q = (-D_q - L_{q-1} g_{q-1} U_{q-1})^-1 with D = H + Sigma - zS, L = hl - z sl,
  * U = hu - z su; backward G_qq, G_{q+1,q}, G_{q,q+1}, G_{q,N}; optional lesser
- * sweep (:121-140).  T(E) (device_property.py:374-406) and the per-orbital DOS
+ * sweep (:121-140) and greater sweep (:143-161).  T(E) (device_property.py:374-406) and the per-orbital DOS
  * diagonal (:408-470) are reduced inside the sweep.  Returns a call-level
  * status; per-item status in p->status. */
 int negf_rgf_run(const NegfRgfProblem* p, void* cuda_stream);

@@ -47,19 +47,19 @@ def test_rgf_matches_reference_fixture(case):
     scalar = bool(g["scalar"])
     E = torch.as_tensor(g["energy"]).cuda()
     seL, seR = torch.as_tensor(g["left_se"]).cuda(), torch.as_tensor(g["right_se"]).cuda()
-    lesser = g.has("s_in")
+    lesser, greater = g.has("s_in"), g.has("s_out")
     kw = dict(eta=float(g["eta"]), E_ref=float(g["E_ref"]), need_gr_lc=g.has("out/gr_lc"))
-    if g.has("s_out"):
-        pytest.skip("G^> sweep is not provided")
     if scalar:
         ans = recursive_gf(E[0], _cu(g["hl"]), _cu(g["hd"]), _cu(g["hu"]), _cu(g["sd"]), _cu(g["su"]),
                            _cu(g["sl"]), seL[0], seR[0],
                            s_in=[torch.as_tensor(s[0]).cuda() for s in g["s_in"]] if lesser else 0,
-                           need_lesser=lesser, **kw)
+                           s_out=[torch.as_tensor(s[0]).cuda() for s in g["s_out"]] if greater else 0,
+                           need_lesser=lesser, need_greater=greater, **kw)
     else:
         ans = recursive_gf(E, _cu(g["hl"]), _cu(g["hd"]), _cu(g["hu"]), _cu(g["sd"]), _cu(g["su"]),
                            _cu(g["sl"]), seL, seR, s_in=_cu(g["s_in"]) if lesser else 0,
-                           need_lesser=lesser, **kw)
+                           s_out=_cu(g["s_out"]) if greater else 0,
+                           need_lesser=lesser, need_greater=greater, **kw)
     _compare(ans, lambda t: g.get("out/" + t))
 
 
@@ -103,6 +103,30 @@ def test_rgf_lesser_matches_oracle():
                          [x.numpy() for x in dev.hu], [x.numpy() for x in dev.sd],
                          [x.numpy() for x in dev.su], [x.numpy() for x in dev.sl],
                          seL.numpy(), seR.numpy(), eta=1e-5, s_in=s_in, need_lesser=True)
+    _compare(ans, lambda t: ref.get(t))
+
+
+@pytest.mark.parametrize("dims,lesser", [([40, 72, 40], False), ([40, 72, 40], True), ([128] * 3, True),
+                                          ([33], False)])
+def test_rgf_greater_matches_oracle(dims, lesser):
+    """G^> sweep (elementwise-conjugate recurrences of recursive_green_cal.py:143-161), alone and
+    next to the lesser sweep in the same launch; Sigma^out = Gamma (1 - f)."""
+    from dpnegf_b200.recursive_green_cal import recursive_gf
+    B = 3
+    dev, seL, seR, E, s_in = _oracle_case(dims, B, seed=13, lesser=True)
+    f = np.linspace(0.1, 0.9, B)
+    s_out = rgf_oracle.s_in_from_se(seL.numpy(), seR.numpy(), 1 - f, f, dims)
+    ans = recursive_gf(E.cuda(), _cu(dev.hl), _cu(dev.hd), _cu(dev.hu), _cu(dev.sd), _cu(dev.su),
+                       _cu(dev.sl), seL.cuda(), seR.cuda(), eta=1e-5, need_lesser=lesser,
+                       s_in=[torch.as_tensor(s).cuda() for s in s_in] if lesser else 0,
+                       need_greater=True, s_out=[torch.as_tensor(s).cuda() for s in s_out])
+    ref = rgf_oracle.rgf(E.numpy(), [x.numpy() for x in dev.hl], [x.numpy() for x in dev.hd],
+                         [x.numpy() for x in dev.hu], [x.numpy() for x in dev.sd],
+                         [x.numpy() for x in dev.su], [x.numpy() for x in dev.sl],
+                         seL.numpy(), seR.numpy(), eta=1e-5, s_in=s_in if lesser else None, s_out=s_out,
+                         need_lesser=lesser, need_greater=True)
+    for t in ("gpd", "gpl", "gpu", "gip_left"):
+        assert ref.get(t) is not None
     _compare(ans, lambda t: ref.get(t))
 
 

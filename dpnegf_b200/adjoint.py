@@ -81,6 +81,39 @@ def transmission(hd: Sequence[torch.Tensor], hu: Sequence[torch.Tensor], hl: Seq
                                  *blocks)
 
 
+def transmission_and_grad(hd: Sequence[torch.Tensor], hu: Sequence[torch.Tensor], hl: Sequence[torch.Tensor],
+                          sd: Sequence[torch.Tensor], su: Sequence[torch.Tensor], sl: Sequence[torch.Tensor],
+                          energy: torch.Tensor, left_se: torch.Tensor, right_se: torch.Tensor,
+                          weights: torch.Tensor, eta: float = 0.0, E_ref: float = 0.0, precision: str = "fp64",
+                          refine: bool = False):
+    """T(E) and the gradient of L = sum_E w_E T(E) for weights known in advance, in one launch.
+
+    The adjoint pass sweeps the device itself and reduces T(E) on the way, so
+    a loss that is linear in T with fixed weights (the Landauer current's
+    Fermi-window quadrature weights, a weighted sum of transmissions) needs no
+    separate forward call: this costs one adjoint launch instead of the
+    forward + backward launches of ``transmission`` under autograd.  Returns
+    ``(T [B], grads)`` with ``grads`` keyed ``hd, hu, hl, sd, su, sl`` (lists
+    of blocks) and ``se_l, se_r`` ([B, n, n], each energy's dL/dSigma), in
+    torch's complex-gradient convention, equal to what autograd through
+    ``transmission`` gives for ``(w * T).sum()``.  ``refine`` refines the
+    column G_{:,N} (mixed precision) before T and the gradient are formed."""
+    K = len(hd)
+    if not (len(sd) == K and len(hu) == len(hl) == len(su) == len(sl) == K - 1):
+        raise ValueError("inconsistent block lists")
+    energy = torch.as_tensor(energy).to(torch.complex128).reshape(-1).detach()
+    w = torch.as_tensor(weights, dtype=torch.float64).reshape(-1).detach()
+    if w.shape[0] != energy.shape[0]:
+        raise ValueError(f"{w.shape[0]} weights for {energy.shape[0]} energies")
+    geom = rgf_plan.Geometry([rgf_plan.DeviceBlocks([t.detach() for t in hd], [t.detach() for t in hu],
+                                                    [t.detach() for t in hl], [t.detach() for t in sd],
+                                                    [t.detach() for t in su], [t.detach() for t in sl])],
+                             device=left_se.device, detect_zero_offdiag=False)
+    res = rgf_plan.run(geom, [energy], [left_se.detach()], [right_se.detach()], eta=eta, E_ref=E_ref, outputs=(),
+                       adjoint_w=w, precision=precision, refine=refine, refine_steps=3 if refine else 1)
+    return res.trans.clone(), res.grads
+
+
 def current(T: torch.Tensor, energy: torch.Tensor, f_left: torch.Tensor, f_right: torch.Tensor) -> torch.Tensor:
     """Landauer current sum(E) (f_L - f_R) T by Simpson's rule (no 2e/h prefactor, as the reference)."""
     e = torch.as_tensor(energy, dtype=torch.float64, device=T.device).real

@@ -121,3 +121,32 @@ def test_current_gradient_chains_through_simpson():
         d[2, 3] = h
         fd = (I(hd1.detach() + d) - I(hd1.detach() - d)).item() / (2 * h)
     assert abs(fd - hd1.grad[2, 3].real.item()) <= 1e-6 * max(1.0, abs(fd))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_fused_value_and_gradient_equals_autograd(precision):
+    """transmission_and_grad (one adjoint launch) gives the forward's T(E) and autograd's gradient of
+    sum w T: equal to rounding for FP64; for mixed, within the mixed path's tolerance."""
+    from dpnegf_b200 import workload
+    from dpnegf_b200.adjoint import transmission, transmission_and_grad
+    dims = [24, 40, 24]
+    dev = workload.random_device(0, 0, seed=31, block_dims=dims)
+    B = 4
+    seL = workload.random_self_energy(B, dims[0], seed=32).cuda()
+    seR = workload.random_self_energy(B, dims[-1], seed=33).cuda()
+    E = torch.linspace(-1.0, 1.0, B, dtype=torch.float64).to(torch.complex128).cuda()
+    w = torch.tensor([0.5, 1.0, -1.5, 2.0], dtype=torch.float64).cuda()
+    blocks = {k: [x.cuda().requires_grad_(True) for x in getattr(dev, k)] for k in ("hd", "hu", "hl", "sd", "su", "sl")}
+    sL, sR = seL.clone().requires_grad_(True), seR.clone().requires_grad_(True)
+    T = transmission(blocks["hd"], blocks["hu"], blocks["hl"], blocks["sd"], blocks["su"], blocks["sl"], E, sL, sR,
+                     eta=1e-5, precision=precision)
+    (w * T).sum().backward()
+    Tf, g = transmission_and_grad(blocks["hd"], blocks["hu"], blocks["hl"], blocks["sd"], blocks["su"],
+                                  blocks["sl"], E, seL, seR, w, eta=1e-5, precision=precision)
+    tol = 1e-12 if precision == "fp64" else 1e-4
+    assert _rel(Tf, T.detach().cpu().numpy()) < tol
+    for k in ("hd", "hu", "hl", "sd", "su", "sl"):
+        for q, x in enumerate(blocks[k]):
+            assert _rel(g[k][q], x.grad.cpu().numpy()) < tol, (k, q)
+    assert _rel(g["se_l"], sL.grad.cpu().numpy()) < tol
+    assert _rel(g["se_r"], sR.grad.cpu().numpy()) < tol

@@ -42,6 +42,7 @@ ADJOINT = 1 << 12
 MIXED = 1 << 13
 REFINE = 1 << 14
 GREATER = 1 << 15
+ADJ_DOS = 1 << 16
 PHASES = ("form", "gemm_fwd", "inv_stage", "inv_panel", "inv_update", "inv_gather", "gemm_bwd", "lesser",
           "dos", "trans", "other", "refine")
 
@@ -55,7 +56,8 @@ DEVICE_DTYPE = np.dtype([("n_blocks", "<i4"), ("blk0", "<i4"), ("n_orb", "<i4"),
                          ("o_gtrans", "<i8"), ("g_slab", "<i8")])
 ITEM_DTYPE = np.dtype([("dev", "<i4"), ("row", "<i4"), ("z_re", "<f8"), ("z_im", "<f8"),
                        ("se_l", "<u8"), ("se_r", "<u8"), ("nse_l", "<i4"), ("nse_r", "<i4"),
-                       ("out", "<i8"), ("orb", "<i8"), ("w_t", "<f8"), ("gse_l", "<u8"), ("gse_r", "<u8")])
+                       ("out", "<i8"), ("orb", "<i8"), ("w_t", "<f8"), ("gse_l", "<u8"), ("gse_r", "<u8"),
+                       ("w_d", "<f8")])
 
 
 LEAD_DTYPE = np.dtype([("n", "<i4"), ("nc", "<i4"), ("b", "<i4"), ("pad", "<i4"), ("h", "<i8"), ("s", "<i8"),

@@ -13,6 +13,18 @@ sweep, the first block row from G_1p = P_p G_pp with P_{p+1} = P_p g_p U_p.
 The re-sweep keeps nothing from the forward call (the extreme of
 checkpointing); one backward costs about 1.7x a forward sweep.
 
+``transmission_dos(...)`` returns T(E) and DOS(E) (the reference's _cal_dos_,
+device_property.py:408-439: -(2/pi) Im Tr[G S] with the block-tridiagonal
+trace), both differentiable: the DOS weighted by occupation x quadrature
+weights is the summed onsite density n, and its gradient comes from a
+z-tangent sweep in the same adjoint launch.  Tr[G S] = d/dz log det(zS - H -
+Sigma), so with Y = G S G = -dG/dz
+  dn/dH_pq = i c conj(Y_qp),  dn/dS_pq = i c (conj(G_qp) - conj(z) conj(Y_qp)),
+  dn/dSigma_pq = i c conj(Y_qp),   c = -(2/pi) w_E,
+and only the block-tridiagonal blocks of Y are needed; the tangent sweep
+differentiates the forward recursion (dg_q = -g_q dK_q g_q) and the backward
+blocks, about 16 more block products per block.
+
 Gradients follow torch's convention for complex leaves (dL/dRe + i dL/dIm),
 so they compose with autograd through the caller's tight-binding model; the
 Landauer current is a differentiable Simpson sum over T (``current``).
@@ -52,6 +64,33 @@ class _TransmissionFn(torch.autograd.Function):
         return (None, None, None, None, None, None, g["se_l"], g["se_r"]) + tuple(block_grads)
 
 
+class _TransmissionDosFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, energy, eta, E_ref, K, precision, left_se, right_se, *blocks):
+        hd, hu, hl, sd, su, sl = _split(blocks, K)
+        geom = rgf_plan.Geometry([rgf_plan.DeviceBlocks(hd, hu, hl, sd, su, sl)], device=left_se.device,
+                                 detect_zero_offdiag=False)
+        res = rgf_plan.run(geom, [energy], [left_se], [right_se], eta=eta, E_ref=E_ref, outputs=(), trans=True,
+                           dos=True, precision=precision)
+        ctx.geom = geom
+        ctx.eta, ctx.E_ref, ctx.K, ctx.precision = eta, E_ref, K, precision
+        ctx.save_for_backward(energy, left_se, right_se)
+        return res.trans.clone(), res.dos.clone()
+
+    @staticmethod
+    def backward(ctx, gT, gD):
+        energy, left_se, right_se = ctx.saved_tensors
+        B = energy.shape[0]
+        z = torch.zeros(B, dtype=torch.float64, device=left_se.device)
+        wt = gT.detach().to(torch.float64) if gT is not None else z
+        wd = gD.detach().to(torch.float64) if gD is not None else z
+        res = rgf_plan.run(ctx.geom, [energy], [left_se], [right_se], eta=ctx.eta, E_ref=ctx.E_ref, outputs=(),
+                           adjoint_w=wt, adjoint_w_dos=wd, precision=ctx.precision)
+        g = res.grads
+        block_grads = g["hd"] + g["hu"] + g["hl"] + g["sd"] + g["su"] + g["sl"]
+        return (None, None, None, None, None, g["se_l"], g["se_r"]) + tuple(block_grads)
+
+
 def _split(blocks, K):
     hd = list(blocks[0:K])
     hu = list(blocks[K:2 * K - 1])
@@ -81,11 +120,28 @@ def transmission(hd: Sequence[torch.Tensor], hu: Sequence[torch.Tensor], hl: Seq
                                  *blocks)
 
 
+def transmission_dos(hd: Sequence[torch.Tensor], hu: Sequence[torch.Tensor], hl: Sequence[torch.Tensor],
+                     sd: Sequence[torch.Tensor], su: Sequence[torch.Tensor], sl: Sequence[torch.Tensor],
+                     energy: torch.Tensor, left_se: torch.Tensor, right_se: torch.Tensor, eta: float = 0.0,
+                     E_ref: float = 0.0, precision: str = "fp64"):
+    """(T(E), DOS(E)), each [B], of one BTD device, both differentiable w.r.t. every
+    2-D block and both ``[B, n, n]`` self-energies (CUDA tensors).  The DOS is the
+    reference's (spin factor 2, block-tridiagonal trace of G S); a weighted sum of
+    it over an energy window is the summed onsite density, so losses such as
+    current + density (Landauer I from T, n from DOS) take one adjoint launch."""
+    K = len(hd)
+    if not (len(sd) == K and len(hu) == len(hl) == len(su) == len(sl) == K - 1):
+        raise ValueError("inconsistent block lists")
+    energy = torch.as_tensor(energy).to(torch.complex128).reshape(-1).detach()
+    blocks = list(hd) + list(hu) + list(hl) + list(sd) + list(su) + list(sl)
+    return _TransmissionDosFn.apply(energy, float(eta), float(E_ref), K, precision, left_se, right_se, *blocks)
+
+
 def transmission_and_grad(hd: Sequence[torch.Tensor], hu: Sequence[torch.Tensor], hl: Sequence[torch.Tensor],
                           sd: Sequence[torch.Tensor], su: Sequence[torch.Tensor], sl: Sequence[torch.Tensor],
                           energy: torch.Tensor, left_se: torch.Tensor, right_se: torch.Tensor,
                           weights: torch.Tensor, eta: float = 0.0, E_ref: float = 0.0, precision: str = "fp64",
-                          refine: bool = False):
+                          refine: bool = False, dos_weights=None):
     """T(E) and the gradient of L = sum_E w_E T(E) for weights known in advance, in one launch.
 
     The adjoint pass sweeps the device itself and reduces T(E) on the way, so
@@ -97,7 +153,9 @@ def transmission_and_grad(hd: Sequence[torch.Tensor], hu: Sequence[torch.Tensor]
     of blocks) and ``se_l, se_r`` ([B, n, n], each energy's dL/dSigma), in
     torch's complex-gradient convention, equal to what autograd through
     ``transmission`` gives for ``(w * T).sum()``.  ``refine`` refines the
-    column G_{:,N} (mixed precision) before T and the gradient are formed."""
+    column G_{:,N} (mixed precision) before T and the gradient are formed.
+    ``dos_weights`` ([B]) add the gradient of sum_E wd_E DOS(E) (the summed
+    onsite density for occupation x quadrature weights) to the same launch."""
     K = len(hd)
     if not (len(sd) == K and len(hu) == len(hl) == len(su) == len(sl) == K - 1):
         raise ValueError("inconsistent block lists")
@@ -109,8 +167,14 @@ def transmission_and_grad(hd: Sequence[torch.Tensor], hu: Sequence[torch.Tensor]
                                                     [t.detach() for t in hl], [t.detach() for t in sd],
                                                     [t.detach() for t in su], [t.detach() for t in sl])],
                              device=left_se.device, detect_zero_offdiag=False)
+    wd = None
+    if dos_weights is not None:
+        wd = torch.as_tensor(dos_weights, dtype=torch.float64).reshape(-1).detach()
+        if wd.shape[0] != energy.shape[0]:
+            raise ValueError(f"{wd.shape[0]} DOS weights for {energy.shape[0]} energies")
     res = rgf_plan.run(geom, [energy], [left_se.detach()], [right_se.detach()], eta=eta, E_ref=E_ref, outputs=(),
-                       adjoint_w=w, precision=precision, refine=refine, refine_steps=3 if refine else 1)
+                       adjoint_w=w, adjoint_w_dos=wd, precision=precision, refine=refine,
+                       refine_steps=3 if refine else 1)
     return res.trans.clone(), res.grads
 
 

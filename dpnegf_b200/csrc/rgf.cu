@@ -47,6 +47,8 @@ struct SlotBufs {
   cplx* yslab;    // refinement: forward-substituted residual y_q of every block
   cplx* gipslab;  // greater gip_q storage when gip_left is not an output
   cplx* Pd;       // greater: gpd_{q+1} when gpd is not an output
+  cplx* gdslab;   // density gradient: z-tangent dg_q/dz of every block
+  cplx *D0, *D1;  // density gradient: dG_qq/dz of the current / next block
   cplx *W, *T1, *Lz, *Uz, *gU, *Gd, *Gl, *Gu, *Gt0, *Gt1, *tA, *tB, *tC, *tD;
   cplx *Nd, *Nl, *Nu, *tE;  // lesser work
 };
@@ -60,6 +62,7 @@ __host__ __device__ inline size_t rgf_slot_elems(const NegfRgfProblem& p) {
   if (p.flags & (NEGF_ADJOINT | NEGF_REFINE)) e += (size_t)p.col_slab;
   if (p.flags & NEGF_REFINE) e += (size_t)p.col_slab;
   if (p.flags & NEGF_GREATER) e += (size_t)p.max_g_slab + mn2;
+  if ((p.flags & NEGF_ADJOINT) && (p.flags & NEGF_ADJ_DOS)) e += (size_t)p.max_g_slab + 2 * mn2;
   return (e + 15) & ~(size_t)15;  // keep slots 256-byte aligned
 }
 constexpr size_t RGF_SCRATCH_HEADER = 256;  // work-queue counter
@@ -81,6 +84,7 @@ NEGF_DEV SlotBufs slot_bufs(const NegfRgfProblem& p, int slot) {
   s.yslab = nullptr;
   s.gipslab = nullptr;
   s.Pd = nullptr;
+  s.gdslab = s.D0 = s.D1 = nullptr;
   if (!(p.flags & NEGF_OUT_GR_LEFT)) { s.gslab = b; b += p.max_g_slab; }
   if (p.flags & NEGF_LESSER) { s.ginslab = b; b += p.max_g_slab; }
   if (p.flags & NEGF_ADJOINT) { s.grdslab = b; b += p.max_g_slab; }
@@ -89,6 +93,11 @@ NEGF_DEV SlotBufs slot_bufs(const NegfRgfProblem& p, int slot) {
   if (p.flags & NEGF_GREATER) {
     s.gipslab = b; b += p.max_g_slab;
     s.Pd = b; b += mn2;
+  }
+  if ((p.flags & NEGF_ADJOINT) && (p.flags & NEGF_ADJ_DOS)) {
+    s.gdslab = b; b += p.max_g_slab;
+    s.D0 = b; b += mn2;
+    s.D1 = b; b += mn2;
   }
   return s;
 }
@@ -250,7 +259,53 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
   const cplx ONE = cmk(1.0, 0.0), MONE = cmk(-1.0, 0.0);
   const bool lesser = (fl & NEGF_LESSER) != 0;
   const bool greater = (fl & NEGF_GREATER) != 0;
+  const bool adj = (fl & NEGF_ADJOINT) != 0;
+  // density gradient of this item: the z-tangent sweep (forward after each inverse,
+  // backward beside the retarded blocks) and the elementwise accumulation below
+  const bool dosg = adj && (fl & NEGF_ADJ_DOS) && it.w_d != 0.0;
   int bad = 0;
+  cplx *gHd = nullptr, *gSd = nullptr, *gHu = nullptr, *gSu = nullptr, *gHl = nullptr, *gSl = nullptr;
+  if (adj) {
+    const int64_t u_slab = (P.grad_slab - 2 * dv.g_slab) / 4;
+    cplx* gslot = reinterpret_cast<cplx*>(P.grad) + (size_t)blockIdx.x * P.grad_slab;
+    gHd = gslot;
+    gSd = gslot + dv.g_slab;
+    gHu = gslot + 2 * dv.g_slab;
+    gSu = gHu + u_slab;
+    gHl = gSu + u_slab;
+    gSl = gHl + u_slab;
+    // the per-item self-energy gradients are sums of the T and density terms
+    cplx* gl = reinterpret_cast<cplx*>(it.gse_l);
+    cplx* gr = reinterpret_cast<cplx*>(it.gse_r);
+    if (gl) for (int e = threadIdx.x; e < it.nse_l * it.nse_l; e += CTA_THREADS) gl[e] = cmk(0.0, 0.0);
+    if (gr) for (int e = threadIdx.x; e < it.nse_r * it.nse_r; e += CTA_THREADS) gr[e] = cmk(0.0, 0.0);
+    __syncthreads();
+  }
+  // Density-gradient weight: DOS = -(2/pi) Im Tr[G S], and with Y = G S G = -dG/dz the
+  // torch-convention gradients of w_d DOS are i c conj(Y_qp)^T for H and Sigma and
+  // i c (-conj(z) conj(Y_qp) + conj(G_qp))^T for S, c = -(2/pi) w_d.
+  const double cd = -0.63661977236758134308 * it.w_d;
+  const cplx zc_d = cconj(z);
+  // gradient block [r x s] += from the tangent Yd = dG/dz and G, both stored [s x r]
+  auto acc_hs = [&](cplx* gH, cplx* gS, const cplx* Yd, const cplx* Gm, int r, int s_) {
+    for (int e = threadIdx.x; e < r * s_; e += CTA_THREADS) {
+      const int i = e / s_, j = e % s_;
+      const cplx y = cconj(Yd[(int64_t)j * r + i]), gg = cconj(Gm[(int64_t)j * r + i]);
+      gH[e] = cadd(gH[e], cmk(cd * y.y, -cd * y.x));  // -i c y
+      const cplx t = cadd(cmul(zc_d, y), gg);
+      gS[e] = cadd(gS[e], cmk(-cd * t.y, cd * t.x));  // i c (conj(z) y + g)
+    }
+  };
+  // self-energy corner [c x c] at (os, os) of gse (ns x ns) from Yd (n x n) at (oy, oy)
+  auto acc_se = [&](double* gse_raw, int ns, int os, const cplx* Yd, int n, int oy, int c) {
+    cplx* gse = reinterpret_cast<cplx*>(gse_raw);
+    for (int e = threadIdx.x; e < c * c; e += CTA_THREADS) {
+      const int i = e / c, j = e % c;
+      const cplx y = cconj(Yd[(int64_t)(oy + j) * n + oy + i]);
+      cplx* d = gse + (int64_t)(os + i) * ns + os + j;
+      *d = cadd(*d, cmk(cd * y.y, -cd * y.x));
+    }
+  };
 
   auto sq = [&](int q) { return (int64_t)blk[q].n * blk[q].n; };
   auto gptr = [&](int q) -> cplx* {
@@ -290,6 +345,23 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
     }
     bad |= cta_inverse<true, MX>(sb.W, nq, nq, gptr(q), nq, smem_raw, &pc, sb.tE,  // tE: pivot-row snapshot
                                  P.inv_ob > 0 ? P.inv_ob : INV_OB);
+    if (dosg) {
+      // dg_q/dz = -g_q Kd g_q with Kd = S_q - (L dg_{q-1} - sl g_{q-1}) U + (L g_{q-1}) su
+      // (d/dz of g_q^-1 = zS_q - H_q - Sigma - L g U, dL/dz = -sl, dU/dz = -su; sb.T1 = L g_{q-1})
+      const cplx* Kd = hs + b.sd;
+      if (q > 0) {
+        const NegfBlock& bp = blk[q - 1];
+        const int np = bp.n;
+        gemm<OP_N, OP_N, MX>(smem, nq, np, np, sb.Lz, np, sb.gdslab + bp.g, np, sb.tA, np);
+        if (bp.sl >= 0) gemm<OP_N, OP_N, MX>(smem, nq, np, np, hs + bp.sl, np, gptr(q - 1), np, sb.tA, np, MONE, sb.tA, np);
+        gemm<OP_N, OP_N, MX>(smem, nq, nq, np, sb.tA, np, sb.Uz, nq, sb.tB, nq, MONE, hs + b.sd, nq);
+        if (bp.su >= 0) gemm<OP_N, OP_N, MX>(smem, nq, nq, np, sb.T1, np, hs + bp.su, nq, sb.tB, nq, ONE, sb.tB, nq);
+        Kd = sb.tB;
+      }
+      gemm<OP_N, OP_N, MX>(smem, nq, nq, nq, gptr(q), nq, Kd, nq, sb.tC, nq);
+      gemm<OP_N, OP_N, MX>(smem, nq, nq, nq, sb.tC, nq, gptr(q), nq, sb.gdslab + b.g, nq, MONE);
+      pc.mark(PH_GEMM_FWD);
+    }
     if (lesser) {
       // gin_q = g_q (s_q + L gin_{q-1} U) g_q^H
       const cplx* s = sinptr(q);
@@ -328,7 +400,6 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
 
   // ----------------------------------------------------------- backward sweep
   const int nN = blk[K - 1].n;
-  const bool adj = (fl & NEGF_ADJOINT) != 0;
   const bool need_gt = (fl & (NEGF_OUT_GTRANS | NEGF_OUT_GR_LC | NEGF_TRANS | NEGF_ORB_AR | NEGF_ADJOINT)) != 0;
   cplx* orbg = (fl & NEGF_ORB_GDIAG) ? reinterpret_cast<cplx*>(P.orb_g) + it.orb : nullptr;
   double* orbar = ((fl & NEGF_ORB_AR) && seR) ? P.orb_ar + it.orb : nullptr;
@@ -399,6 +470,17 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
     __syncthreads();
     spectral_diag(orbar + blk[K - 1].orb0, gt, nN);
   }
+  const cplx* Dnext = nullptr;  // dG_{q+1,q+1}/dz
+  int dtog = 0;
+  if (dosg) {
+    Dnext = sb.gdslab + blk[K - 1].g;
+    acc_hs(gHd + blk[K - 1].g, gSd + blk[K - 1].g, Dnext, gptr(K - 1), nN, nN);
+    if (seR && it.gse_r) {
+      const int crd = min(nN, it.nse_r);
+      acc_se(it.gse_r, it.nse_r, it.nse_r - crd, Dnext, nN, nN - crd, crd);
+    }
+    __syncthreads();
+  }
   int tog = 0;
   for (int q = K - 2; q >= 0; --q) {
     const NegfBlock& b = blk[q];
@@ -423,6 +505,29 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
       gemm<OP_N, OP_N, MX>(smem, nq, nN, nn, sb.gU, nn, gt, nN, gtn, nN);
       gt = gtn;
       tog ^= 1;
+    }
+    if (dosg) {
+      // z-tangents of the retarded blocks (Gnext = G_{q+1,q+1}, sb.T1 = Gnext L, sb.gU = g U):
+      //   gUd = dg U - g su;  T1d = Dnext L - Gnext sl;  dgrl = T1d g + T1 dg;
+      //   dgru = gUd Gnext + gU Dnext;  dgrd = dg + gUd grl + gU dgrl
+      const cplx* dg = sb.gdslab + b.g;
+      cplx* Dcur = dtog ? sb.D1 : sb.D0;
+      gemm<OP_N, OP_N, MX>(smem, nq, nn, nq, dg, nq, sb.Uz, nn, sb.tA, nn);
+      if (b.su >= 0) gemm<OP_N, OP_N, MX>(smem, nq, nn, nq, g, nq, hs + b.su, nn, sb.tA, nn, MONE, sb.tA, nn);
+      gemm<OP_N, OP_N, MX>(smem, nn, nq, nn, Dnext, nn, sb.Lz, nq, sb.tB, nq);
+      if (b.sl >= 0) gemm<OP_N, OP_N, MX>(smem, nn, nq, nn, Gnext, nn, hs + b.sl, nq, sb.tB, nq, MONE, sb.tB, nq);
+      gemm<OP_N, OP_N, MX>(smem, nn, nq, nq, sb.tB, nq, g, nq, sb.tC, nq);
+      gemm<OP_N, OP_N, MX>(smem, nn, nq, nq, sb.T1, nq, dg, nq, sb.tC, nq, ONE, sb.tC, nq);
+      gemm<OP_N, OP_N, MX>(smem, nq, nn, nn, sb.tA, nn, Gnext, nn, sb.tD, nn);
+      gemm<OP_N, OP_N, MX>(smem, nq, nn, nn, sb.gU, nn, Dnext, nn, sb.tD, nn, ONE, sb.tD, nn);
+      gemm<OP_N, OP_N, MX>(smem, nq, nq, nn, sb.tA, nn, grl, nq, Dcur, nq, ONE, dg, nq);
+      gemm<OP_N, OP_N, MX>(smem, nq, nq, nn, sb.gU, nn, sb.tC, nq, Dcur, nq, ONE, Dcur, nq);
+      acc_hs(gHd + b.g, gSd + b.g, Dcur, grd, nq, nq);         // (q, q)
+      acc_hs(gHu + b.gu, gSu + b.gu, sb.tC, grl, nq, nn);      // (q, q+1): Y_{q+1,q}, G_{q+1,q}
+      acc_hs(gHl + b.gu, gSl + b.gu, sb.tD, gru, nn, nq);      // (q+1, q): Y_{q,q+1}, G_{q,q+1}
+      __syncthreads();
+      Dnext = Dcur;
+      dtog ^= 1;
     }
     pc.mark(PH_GEMM_BWD);
     if (orbg) gdiag(orbg + b.orb0, grd, nq);
@@ -493,6 +598,10 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
       pc.mark(PH_DOS);
     }
     Gnext = grd;
+  }
+  if (dosg && seL && it.gse_l) {  // Dnext = dG_11/dz
+    acc_se(it.gse_l, it.nse_l, 0, Dnext, blk[0].n, 0, min(blk[0].n, it.nse_l));
+    __syncthreads();
   }
   if (fl & NEGF_OUT_GTRANS) {
     cplx* d = out + dv.o_gtrans + row * (int64_t)blk[0].n * nN;
@@ -605,19 +714,11 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
   // d(c T)/dX_pq = 2c W_qp^H with W_qp = G_qN M G_1p, M = Gamma_R G_1N^H Gamma_L
   // restricted to the lead corners: W_qp = R_q (M_c F_p), R_q = G_qN[:, nN-cr:],
   // F_p = G_1p[0:cl, :] = P_p G_pp, P_{p+1} = P_p g_p U_p, P_0 = I (rows 0..cl).
-  if (adj && seL && seR) {
+  if (adj && seL && seR && it.w_t != 0.0) {
     const int n0 = blk[0].n;
     const int cl = min(n0, it.nse_l), cr = min(nN, it.nse_r);
     const double c2 = 2.0 * it.w_t;
     const cplx zc = cconj(z);
-    const int64_t u_slab = (P.grad_slab - 2 * dv.g_slab) / 4;
-    cplx* gslot = reinterpret_cast<cplx*>(P.grad) + (size_t)blockIdx.x * P.grad_slab;
-    cplx* gHd = gslot;
-    cplx* gSd = gslot + dv.g_slab;
-    cplx* gHu = gslot + 2 * dv.g_slab;
-    cplx* gSu = gHu + u_slab;
-    cplx* gHl = gSu + u_slab;
-    cplx* gSl = gHl + u_slab;
     const cplx* Gc = gt + (nN - cr);  // G_1N[0:cl, nN-cr:], row stride nN
     cplx* Mc = sb.tE;                 // cr x cl
     gemm<OP_N, OP_C, MX>(smem, cr, cl, cr, sb.tB, cr, Gc, nN, sb.T1, cl);   // Gamma_R Gc^H
@@ -635,7 +736,7 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
           cplx k = sb.Nd[(int64_t)i * cl + j];
           v = cmk(c2 * k.y, -c2 * k.x);  // -2ic k
         }
-        gseL[e] = v;
+        gseL[e] = cadd(gseL[e], v);
       }
     }
     if (gseR) {
@@ -648,7 +749,7 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
           cplx k = sb.Nl[(int64_t)(i - o) * cr + (j - o)];
           v = cmk(c2 * k.y, -c2 * k.x);
         }
-        gseR[e] = v;
+        gseR[e] = cadd(gseR[e], v);
       }
     }
     __syncthreads();
@@ -776,6 +877,7 @@ int negf_rgf_run(const NegfRgfProblem* p, void* stream) {
       (!p->grad || p->grad_slab <= 0 || p->col_slab <= 0 || !(p->flags & NEGF_TRANS)))
     return NEGF_ERR_ARGUMENT;
   if ((p->flags & NEGF_REFINE) && (p->col_slab <= 0 || !(p->flags & NEGF_TRANS))) return NEGF_ERR_ARGUMENT;
+  if ((p->flags & NEGF_ADJ_DOS) && !(p->flags & NEGF_ADJOINT)) return NEGF_ERR_ARGUMENT;
   if (p->inv_ob != 0 && p->inv_ob != 32 && p->inv_ob != 64 && p->inv_ob != 128 && p->inv_ob != 256 &&
       p->inv_ob != 512)
     return NEGF_ERR_ARGUMENT;

@@ -208,7 +208,7 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
         trans=False, orb_dos=False, dos=False, orb_g=False, orb_ar=False,
         s_in: Optional[List[List[Optional[torch.Tensor]]]] = None,
         s_out: Optional[List[List[Optional[torch.Tensor]]]] = None,
-        n_slots=None, check=True, stream=None, phase=False, events=None, adjoint_w=None,
+        n_slots=None, check=True, stream=None, phase=False, events=None, adjoint_w=None, adjoint_w_dos=None,
         precision="fp64", refine=False, refine_steps=1, defer=False, inv_ob=None):
     """Run the batched sweep.
 
@@ -223,6 +223,9 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     ``adjoint_w`` ([B] weights of T(E), single device) switches the adjoint
     on: the result carries d(sum w T)/d(hd, hu, hl, sd, su, sl) and per-energy
     dT/dSigma_L, dT/dSigma_R weighted by w (torch's complex convention).
+    ``adjoint_w_dos`` ([B] weights of DOS(E), with or without ``adjoint_w``)
+    adds the gradient of sum w_d DOS to the same results: the summed onsite
+    density over the energies when the weights are occupation x quadrature.
     ``precision="mixed"`` runs every block product on the tcgen05 3xTF32 GEMM
     (FP32-accurate products; pivoting, panels and storage stay FP64);
     ``refine=True`` (with ``trans``) adds ``refine_steps`` FP64-residual
@@ -270,7 +273,9 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
         flags |= _lib.LESSER
     if greater:
         flags |= _lib.GREATER
-    adjoint = adjoint_w is not None
+    adjoint = adjoint_w is not None or adjoint_w_dos is not None
+    if adjoint_w_dos is not None:
+        flags |= _lib.ADJ_DOS
     if adjoint:
         if nd != 1:
             raise ValueError("the adjoint runs on a single device")
@@ -369,8 +374,10 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
         rows = np.arange(B, dtype=np.int64)
         it = np.zeros(B, dtype=_lib.ITEM_DTYPE)
         if adjoint:
-            w = torch.as_tensor(adjoint_w, dtype=torch.float64).reshape(-1).cpu().numpy()
-            it["w_t"] = w
+            if adjoint_w is not None:
+                it["w_t"] = torch.as_tensor(adjoint_w, dtype=torch.float64).reshape(-1).cpu().numpy()
+            if adjoint_w_dos is not None:
+                it["w_d"] = torch.as_tensor(adjoint_w_dos, dtype=torch.float64).reshape(-1).cpu().numpy()
             gseL_t = torch.empty((B, nsl, nsl), dtype=C128, device=dev) if nsl else None
             gseR_t = torch.empty((B, nsr, nsr), dtype=C128, device=dev) if nsr else None
             keep_alive += [x for x in (gseL_t, gseR_t) if x is not None]

@@ -64,6 +64,10 @@ extern "C" {
                                       G_{:,N} before T(E) -- FP64 residual E_N - (zS - H - Sigma) G_{:,N} on
                                       FP64 tensor cores, correction solved with the stored g_q (needs
                                       col_slab); gr_lc outputs carry the refined column */
+#define NEGF_ADJ_DOS (1u << 16)    /* with NEGF_ADJOINT: also accumulate the gradient of sum_items w_d DOS(E)
+                                      (the summed onsite density over the items' energies, DOS as in
+                                      NEGF_DOS) by a z-tangent sweep: Tr[G S] = d/dz log det(zS - H - Sigma),
+                                      so the gradient needs the BTD blocks of G S G = -dG/dz */
 #define NEGF_GREATER (1u << 15)    /* greater sweep from s_out: gip_left, gpd, gpl, gpu
                                       (recursive_green_cal.py:143-161, :267-289) */
 
@@ -117,6 +121,7 @@ typedef struct NegfItem {
   double w_t;      /* NEGF_ADJOINT: weight of this item's T(E) in the loss */
   double* gse_l;   /* NEGF_ADJOINT: d loss / d Sigma_L [nse_l x nse_l] (torch convention); NULL = skip */
   double* gse_r;   /* NEGF_ADJOINT: d loss / d Sigma_R [nse_r x nse_r]; NULL = skip */
+  double w_d;      /* NEGF_ADJ_DOS: weight of this item's DOS(E) in the loss */
 } NegfItem;
 
 typedef struct NegfRgfProblem {

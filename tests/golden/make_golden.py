@@ -19,7 +19,11 @@ seeded inputs together with the reference's own outputs:
                   (negf/negf_utils.py:136);
   adjoint_*.npz   gradients of sum_E w_E T(E) w.r.t. every H/S block and both
                   self-energies by torch autograd through the reference
-                  ``recursive_gf`` (T as in ``_cal_tc_``, device_property.py:374-406).
+                  ``recursive_gf`` (T as in ``_cal_tc_``, device_property.py:374-406);
+  adjoint_dos_*.npz  the same for sum_E (wT_E T(E) + wD_E DOS(E)), the DOS formed
+                  from the reference's blocks as ``_cal_dos_`` does
+                  (device_property.py:408-439): the summed onsite density over
+                  an energy window when wD carries occupation x quadrature weights.
 The fixtures are small (tens of KB) and are committed; the GPU box never needs
 the reference sources.
 """
@@ -252,6 +256,52 @@ def _adjoint_case(rgf_mod, name, dims, B, seed, eta=1e-5):
     np.savez_compressed(os.path.join(HERE, f"adjoint_{name}.npz"), **d)
 
 
+def _adjoint_dos_case(rgf_mod, name, dims, B, seed, with_t, eta=1e-5):
+    dev = workload.random_device(0, 0, seed=seed, block_dims=dims)
+    leaf = lambda xs: [x.clone().requires_grad_(True) for x in xs]
+    hd, hu, hl, sd, su, sl = (leaf(getattr(dev, k)) for k in ("hd", "hu", "hl", "sd", "su", "sl"))
+    seL = workload.random_self_energy(B, dims[0], seed=seed + 1).requires_grad_(True)
+    seR = workload.random_self_energy(B, dims[-1], seed=seed + 2).requires_grad_(True)
+    E = torch.linspace(-1.1, 0.9, B, dtype=torch.float64).to(torch.complex128)
+    wT = torch.linspace(0.5, 1.5, B, dtype=torch.float64) if with_t else torch.zeros(B, dtype=torch.float64)
+    wD = torch.linspace(1.0, -0.5, B, dtype=torch.float64)
+    ans = rgf_mod.recursive_gf(E, hl=hl, hd=hd, hu=hu, sd=sd, su=su, sl=sl, left_se=seL, right_se=seR, eta=eta)
+    G, grd, grl, gru = ans[0], ans[2], ans[3], ans[4]
+    gL = 1j * (seL - seL.mH)
+    gR = 1j * (seR - seR.mH)
+    T = (gL @ G @ gR @ G.mH).diagonal(dim1=-2, dim2=-1).real.sum(-1)
+    dos = 0
+    K = len(grd)
+    for j in range(K):  # _cal_dos_ (device_property.py:430-439)
+        if K == 1:
+            t = grd[j] @ sd[j]
+        elif j == 0:
+            t = grd[j] @ sd[j] + gru[j] @ sl[j]
+        elif j == K - 1:
+            t = grd[j] @ sd[j] + grl[j - 1] @ su[j - 1]
+        else:
+            t = grd[j] @ sd[j] + grl[j - 1] @ su[j - 1] + gru[j] @ sl[j]
+        dos = dos - t.imag.diagonal(dim1=-2, dim2=-1).sum(-1) / np.pi
+    dos = 2 * dos
+    ((wT * T).sum() + (wD * dos).sum()).backward()
+    d = {}
+    _put(d, "dims", np.array(dims))
+    _put(d, "energy", E)
+    _put(d, "eta", np.array(eta))
+    _put(d, "w", wT)
+    _put(d, "wd", wD)
+    _put(d, "T", T.detach())
+    _put(d, "dos", dos.detach())
+    for k, v in (("hd", hd), ("hu", hu), ("hl", hl), ("sd", sd), ("su", su), ("sl", sl)):
+        _put(d, k, [x.detach() for x in v])
+        _put(d, "grad/" + k, [x.grad for x in v])
+    _put(d, "left_se", seL.detach())
+    _put(d, "right_se", seR.detach())
+    _put(d, "grad/left_se", seL.grad)
+    _put(d, "grad/right_se", seR.grad)
+    np.savez_compressed(os.path.join(HERE, f"adjoint_dos_{name}.npz"), **d)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default=ref_import.DEFAULT_REF_ROOT)
@@ -285,6 +335,9 @@ def main():
         _adjoint_case(rgf_mod, "nonuniform", [6, 9, 5, 7], 3, seed=21)
         _adjoint_case(rgf_mod, "uniform", [10] * 5, 2, seed=22)
         _adjoint_case(rgf_mod, "single_block", [8], 2, seed=23)
+        _adjoint_dos_case(rgf_mod, "nonuniform", [6, 9, 5, 7], 3, seed=24, with_t=False)
+        _adjoint_dos_case(rgf_mod, "uniform_with_t", [10] * 5, 2, seed=25, with_t=True)
+        _adjoint_dos_case(rgf_mod, "single_block", [8], 2, seed=26, with_t=False)
     print("golden fixtures written to", HERE)
 
 

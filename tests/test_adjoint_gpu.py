@@ -150,3 +150,101 @@ def test_fused_value_and_gradient_equals_autograd(precision):
             assert _rel(g[k][q], x.grad.cpu().numpy()) < tol, (k, q)
     assert _rel(g["se_l"], sL.grad.cpu().numpy()) < tol
     assert _rel(g["se_r"], sR.grad.cpu().numpy()) < tol
+
+
+@pytest.mark.parametrize("case", ["adjoint_dos_nonuniform", "adjoint_dos_uniform_with_t", "adjoint_dos_single_block"])
+def test_density_gradients_match_reference_autograd(case):
+    """Gradient of sum wT T + sum wD DOS (DOS as the reference's _cal_dos_) against torch autograd
+    through the reference recursive_gf (fixtures; the first and last cases have wT = 0)."""
+    from dpnegf_b200.adjoint import transmission_dos
+    g = Golden(case)
+    b, seL, seR = _inputs(g)
+    E = torch.as_tensor(g["energy"]).cuda()
+    T, D = transmission_dos(b["hd"], b["hu"], b["hl"], b["sd"], b["su"], b["sl"], E, seL, seR, eta=float(g["eta"]))
+    assert _rel(T, g["T"]) < 1e-10
+    assert _rel(D, g["dos"]) < 1e-10
+    wT = torch.as_tensor(g["w"]).cuda()
+    wD = torch.as_tensor(g["wd"]).cuda()
+    ((wT * T).sum() + (wD * D).sum()).backward()
+    for k in ("hd", "hu", "hl", "sd", "su", "sl"):
+        for q, (x, ref) in enumerate(zip(b[k], g["grad/" + k])):
+            assert _rel(x.grad, ref) < 1e-9, (k, q, _rel(x.grad, ref))
+    assert _rel(seL.grad, g["grad/left_se"]) < 1e-9
+    assert _rel(seR.grad, g["grad/right_se"]) < 1e-9
+
+
+def test_density_gradient_matches_finite_differences():
+    """Central differences (h = 1e-6) of the CUDA DOS on random H, S and Sigma entries."""
+    from dpnegf_b200 import workload
+    from dpnegf_b200.adjoint import transmission_dos
+    dims = [14, 10, 16]
+    dev = workload.random_device(0, 0, seed=15, block_dims=dims)
+    B = 3
+    seL = workload.random_self_energy(B, dims[0], seed=16).cuda()
+    seR = workload.random_self_energy(B, dims[-1], seed=17).cuda()
+    E = torch.tensor([-0.6, 0.2, 1.1], dtype=torch.complex128).cuda()
+    wD = torch.tensor([0.7, -1.2, 0.4], dtype=torch.float64).cuda()
+    blocks = {k: [x.cuda().requires_grad_(True) for x in getattr(dev, k)] for k in ("hd", "hu", "hl", "sd", "su", "sl")}
+    seLr = seL.clone().requires_grad_(True)
+    seRr = seR.clone().requires_grad_(True)
+
+    def loss(bl, sL, sR):
+        _, D = transmission_dos(bl["hd"], bl["hu"], bl["hl"], bl["sd"], bl["su"], bl["sl"], E, sL, sR, eta=1e-5)
+        return (wD * D).sum()
+
+    loss(blocks, seLr, seRr).backward()
+    rng = np.random.default_rng(1)
+    h = 1e-6
+    with torch.no_grad():
+        base = {k: [x.detach().clone() for x in v] for k, v in blocks.items()}
+        for name, q in (("hd", 0), ("hd", 2), ("hu", 1), ("hl", 0), ("sd", 1), ("su", 0), ("sl", 1)):
+            X = base[name][q]
+            for _ in range(2):
+                i, j = rng.integers(X.shape[0]), rng.integers(X.shape[1])
+                for part, unit in (("re", 1.0), ("im", 1j)):
+                    def shifted(s):
+                        bl = {k: [x.clone() for x in v] for k, v in base.items()}
+                        bl[name][q][i, j] += s * unit
+                        return loss(bl, seL, seR).item()
+                    fd = (shifted(h) - shifted(-h)) / (2 * h)
+                    gr = blocks[name][q].grad[i, j]
+                    ad = gr.real.item() if part == "re" else gr.imag.item()
+                    assert abs(fd - ad) <= 1e-5 * max(1.0, abs(ad)), (name, q, i, j, part, fd, ad)
+        for which, S, gradS in (("L", seL, seLr.grad), ("R", seR, seRr.grad)):
+            e, i, j = rng.integers(B), rng.integers(S.shape[1]), rng.integers(S.shape[2])
+            for part, unit in (("re", 1.0), ("im", 1j)):
+                def shifted(s):
+                    S2 = S.clone()
+                    S2[e, i, j] += s * unit
+                    return loss(base, S2, seR).item() if which == "L" else loss(base, seL, S2).item()
+                fd = (shifted(h) - shifted(-h)) / (2 * h)
+                gr = gradS[e, i, j]
+                ad = gr.real.item() if part == "re" else gr.imag.item()
+                assert abs(fd - ad) <= 1e-5 * max(1.0, abs(ad)), (which, e, i, j, part, fd, ad)
+
+
+def test_fused_current_and_density_gradient_equals_autograd():
+    """One adjoint launch for sum wT T + sum wD DOS equals autograd through transmission_dos."""
+    from dpnegf_b200 import workload
+    from dpnegf_b200.adjoint import transmission_and_grad, transmission_dos
+    dims = [32, 32, 32, 32]
+    dev = workload.random_device(0, 0, seed=41, block_dims=dims)
+    B = 4
+    seL = workload.random_self_energy(B, 32, seed=42).cuda()
+    seR = workload.random_self_energy(B, 32, seed=43).cuda()
+    E = torch.linspace(-0.8, 0.8, B, dtype=torch.float64).to(torch.complex128).cuda()
+    wT = torch.tensor([1.0, 0.5, -0.25, 2.0], dtype=torch.float64).cuda()
+    wD = torch.tensor([0.3, 0.3, 0.3, 0.3], dtype=torch.float64).cuda()
+    blocks = {k: [x.cuda().requires_grad_(True) for x in getattr(dev, k)] for k in ("hd", "hu", "hl", "sd", "su", "sl")}
+    sL, sR = seL.clone().requires_grad_(True), seR.clone().requires_grad_(True)
+    T, D = transmission_dos(blocks["hd"], blocks["hu"], blocks["hl"], blocks["sd"], blocks["su"], blocks["sl"],
+                            E, sL, sR, eta=1e-5)
+    ((wT * T).sum() + (wD * D).sum()).backward()
+    Tf, g = transmission_and_grad(blocks["hd"], blocks["hu"], blocks["hl"], blocks["sd"], blocks["su"],
+                                  blocks["sl"], E, seL, seR, wT, eta=1e-5, dos_weights=wD)
+    assert _rel(Tf, T.detach().cpu().numpy()) < 1e-12
+    for k in ("hd", "hu", "hl", "sd", "su", "sl"):
+        for q, x in enumerate(blocks[k]):
+            assert _rel(g[k][q], x.grad.cpu().numpy()) < 1e-12, (k, q)
+    assert _rel(g["se_l"], sL.grad.cpu().numpy()) < 1e-12
+    assert _rel(g["se_r"], sR.grad.cpu().numpy()) < 1e-12

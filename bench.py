@@ -244,6 +244,55 @@ def torch_reference_leg(torch, dev, E, seL, seR, eta, n_energies, chunk=32):
     return T, idx, ms
 
 
+def current_density_leg(torch, rgf_plan, workload, eta):
+    """Gradient cost of the current + density loss: b=96, L=32, 1024 energies in [-0.3, 0.3] eV.
+
+    Loss = I + n with I = sum_E w_E T(E), w_E the trapezoid weights of the Landauer window
+    f_L - f_R at V = 0.3 V, kT = 25 meV, and n = sum_E v_E DOS(E), v_E = f(E) x trapezoid weight
+    (the occupied part of the window).  Forward = one T + DOS sweep; gradient = the one adjoint
+    launch returning T and d(I + n)/d(every H, S block, both self-energies).  Both precisions,
+    one warm-up and one timed call each (CUDA events)."""
+    b, L, nE = 96, 32, 1024
+    d = workload.random_device(b, L, seed=4242)
+    geom = rgf_plan.Geometry([rgf_plan.DeviceBlocks(d.hd, d.hu, d.hl, d.sd, d.su, d.sl)])
+    E = torch.linspace(-0.3, 0.3, nE, dtype=torch.float64)
+    seL = workload.random_self_energy(nE, b, seed=4243).cuda()
+    seR = workload.random_self_energy(nE, b, seed=4244).cuda()
+    dx = float(E[1] - E[0])
+    tw = torch.full((nE,), dx, dtype=torch.float64)
+    tw[0] = tw[-1] = dx / 2
+    kT, V = 0.025, 0.3
+    fL = 1 / (1 + torch.exp((E - V / 2) / kT))
+    fR = 1 / (1 + torch.exp((E + V / 2) / kT))
+    wI = (fL - fR) * tw
+    wn = 0.5 * (fL + fR) * tw
+    Ez = E.to(torch.complex128).cuda()
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        a, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b_.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b_)
+
+    out = {}
+    for prec in ("fp64", "mixed"):
+        tf = timed(lambda: rgf_plan.run(geom, [Ez], [seL], [seR], eta=eta, outputs=(), trans=True, dos=True,
+                                        check=False, precision=prec))
+        tg = timed(lambda: rgf_plan.run(geom, [Ez], [seL], [seR], eta=eta, outputs=(), check=False,
+                                        adjoint_w=wI, adjoint_w_dos=wn, precision=prec))
+        out[prec] = {"forward_value": nE / (tf * 1e-3), "grad_value": nE / (tg * 1e-3), "grad_over_forward": tg / tf,
+                     "unit": UNIT}
+    out["note"] = ("config-4 loss I + n (Landauer current by trapezoid weights at V=0.3 V, kT=25 meV, plus the "
+                   "occupied summed onsite density); grad_value = energy points/s of T plus the full gradient "
+                   "from one adjoint launch (T adjoint + z-tangent density pass); grad_over_forward = that "
+                   "launch / a T+DOS forward launch")
+    return out
+
+
 def traffic_per_point(b, L):
     """DRAM bytes per energy point from the committed ncu summary, scaled by block count."""
     path = os.path.join(ROOT, "profiles", "rgf_kernel_traffic.json")
@@ -464,6 +513,7 @@ def main():
                              "forward_value": B / (tf * 1e-3), "grad_over_forward": ta / tf,
                              "fused_value": B / (ta * 1e-3)}
         adjoint["mixed_vs_fp64"] = adjoint["mixed"]["value"] / adjoint["fp64"]["value"]
+        adjoint["current_density_b96_L32"] = current_density_leg(torch, rgf_plan, workload, args.eta)
         adjoint["note"] = ("value = energy points/s of T(E) plus the full gradient d(sum T)/d(all H, S "
                            "blocks, both self-energies) through autograd (forward launch + adjoint launch); "
                            "fused_value = the same T(E) and gradient from the single adjoint launch "

@@ -248,3 +248,26 @@ def test_fused_current_and_density_gradient_equals_autograd():
             assert _rel(g[k][q], x.grad.cpu().numpy()) < 1e-12, (k, q)
     assert _rel(g["se_l"], sL.grad.cpu().numpy()) < 1e-12
     assert _rel(g["se_r"], sR.grad.cpu().numpy()) < 1e-12
+
+
+def test_mixed_density_gradient_close_to_fp64():
+    """The mixed-precision (3xTF32 products) current + density gradient stays within the mixed
+    path's block tolerance (1e-3 relative) of the FP64 one on a short chain."""
+    from dpnegf_b200 import workload
+    from dpnegf_b200.adjoint import transmission_and_grad
+    dims = [48, 48, 48]
+    dev = workload.random_device(0, 0, seed=51, block_dims=dims)
+    B = 3
+    seL = workload.random_self_energy(B, 48, seed=52).cuda()
+    seR = workload.random_self_energy(B, 48, seed=53).cuda()
+    E = torch.tensor([-0.4, 0.1, 0.5], dtype=torch.complex128).cuda()
+    wT = torch.tensor([1.0, 1.0, 1.0], dtype=torch.float64).cuda()
+    wD = torch.tensor([0.5, 0.5, 0.5], dtype=torch.float64).cuda()
+    blocks = {k: [x.cuda() for x in getattr(dev, k)] for k in ("hd", "hu", "hl", "sd", "su", "sl")}
+    args = (blocks["hd"], blocks["hu"], blocks["hl"], blocks["sd"], blocks["su"], blocks["sl"], E, seL, seR, wT)
+    T64, g64 = transmission_and_grad(*args, eta=1e-5, dos_weights=wD)
+    Tmx, gmx = transmission_and_grad(*args, eta=1e-5, dos_weights=wD, precision="mixed")
+    assert _rel(Tmx, T64.cpu().numpy()) < 1e-3
+    for k in ("hd", "hu", "hl", "sd", "su", "sl"):
+        for q in range(len(g64[k])):
+            assert _rel(gmx[k][q], g64[k][q].cpu().numpy()) < 1e-3, (k, q)

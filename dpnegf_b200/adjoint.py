@@ -178,6 +178,114 @@ def transmission_and_grad(hd: Sequence[torch.Tensor], hu: Sequence[torch.Tensor]
     return res.trans.clone(), res.grads
 
 
+class _LeadSelfEnergyFn(torch.autograd.Function):
+    """Sigma(E) of one lead, differentiable through the converged decimation fixed point.
+
+    Forward: the CUDA Lopez-Sancho decimation (one launch for every energy) gives
+    g_s and Sigma.  Backward: g_s is the fixed point of
+        f(g) = (z S - H - tau g tau')^-1,  tau = z S01 - H01,  tau' = z S01^H - H01^H
+    (the residual the reference checks, negf/surface_green.py:142-145), so with
+    V = dL/dg_s (from Sigma = (E S_DL - H_DL) g_s[:b,:b] (E S_DL^H - H_DL^H), or the
+    bulk form (E S - H) - g_s^-1) the implicit-function adjoint is
+        Lambda = V + P^H Lambda Q^H,   P = g_s tau,  Q = tau' g_s,
+    a Stein equation solved by doubling (Lambda += A Lambda B, A <- A^2, B <- B^2:
+    2^j terms after j steps, the Lopez-Sancho convergence, since the spectral
+    radii of P and Q are below one for eta > 0), and dL/dtheta is the
+    vector-Jacobian product of f at the fixed point with Lambda (torch autograd
+    of one evaluation of f, batched over energies on the GPU), plus the explicit
+    dependence of Sigma on H_DL, S_DL, H and S."""
+
+    @staticmethod
+    def forward(ctx, energies, eta, E_ref, bulk, hL, hLL, sL, sLL, hDL, sDL):
+        from . import surface_green as sg
+        lead = sg.LeadBlocks(hL=hL.detach(), hLL=hLL.detach(), sL=sL.detach(), sLL=sLL.detach(),
+                             hDL=None if hDL is None else hDL.detach(), sDL=None if sDL is None else sDL.detach())
+        arena = sg.LeadArena([lead], device=hL.device)
+        E = energies.detach().cpu().numpy()
+        res = sg.self_energies(arena, [0] * len(E), E, eta, E_ref=E_ref, want_gs=True)
+        gs = torch.stack(res.gs)
+        sig = torch.stack(res.sigma)
+        if hDL is None and bulk:
+            Eb = (energies.to(hL.device) + E_ref).view(-1, 1, 1)
+            sig = Eb * sL.detach() - hL.detach() - sig
+        ctx.save_for_backward(energies, gs, hL, hLL, sL, sLL, hDL, sDL)
+        ctx.eta, ctx.E_ref, ctx.bulk = eta, E_ref, bulk
+        return sig
+
+    @staticmethod
+    def backward(ctx, gsig):
+        energies, gs, hL, hLL, sL, sLL, hDL, sDL = ctx.saved_tensors
+        dev = hL.device
+        E = (energies.to(dev) + ctx.E_ref).view(-1, 1, 1)
+        z = E + 1j * ctx.eta
+        with torch.enable_grad():
+            th = [t.detach().requires_grad_(True) for t in (hL, hLL, sL, sLL)]
+            tHL, tHLL, tSL, tSLL = th
+            dl = [None if t is None else t.detach().requires_grad_(True) for t in (hDL, sDL)]
+            g = gs.detach().requires_grad_(True)
+            if hDL is not None:
+                b = hDL.shape[-1]
+                sdl = dl[1] if dl[1] is not None else torch.zeros_like(dl[0])
+                sig = (E * sdl - dl[0]) @ g[:, :b, :b] @ (E * sdl.mH - dl[0].mH)
+            elif ctx.bulk:
+                sig = torch.linalg.inv(g)
+            else:
+                sig = E * tSL - tHL - torch.linalg.inv(g)
+            ins = [g] + th + [t for t in dl if t is not None]
+            grads = torch.autograd.grad(sig, ins, grad_outputs=gsig, allow_unused=True)
+            V = grads[0]
+            # adjoint of the fixed point: Lambda = V + P^H Lambda Q^H by doubling
+            tau = z * tSLL.detach() - tHLL.detach()
+            taup = z * tSLL.detach().mH - tHLL.detach().mH
+            A = (gs @ tau).mH
+            B = (taup @ gs).mH
+            lam = V
+            for _ in range(64):
+                lam = lam + A @ lam @ B
+                A = A @ A
+                B = B @ B
+                if float(A.abs().amax()) * float(B.abs().amax()) < 1e-32:
+                    break
+            fval = torch.linalg.inv(z * tSL - tHL - (z * tSLL - tHLL) @ gs.detach() @ (z * tSLL.mH - tHLL.mH))
+            gth = torch.autograd.grad(fval, th, grad_outputs=lam, allow_unused=True)
+        out = []
+        for i in range(4):
+            a_ = grads[1 + i]
+            b_ = gth[i]
+            if a_ is None and b_ is None:
+                out.append(None)
+            else:
+                out.append((a_ if a_ is not None else 0) + (b_ if b_ is not None else 0))
+        k = 5
+        gdl = []
+        for t in dl:
+            if t is None:
+                gdl.append(None)
+            else:
+                gdl.append(grads[k])
+                k += 1
+        return (None, None, None, None) + tuple(out) + tuple(gdl)
+
+
+def lead_self_energy(hL: torch.Tensor, hLL: torch.Tensor, sL: torch.Tensor, sLL: torch.Tensor,
+                     energies: torch.Tensor, eta: float, hDL: torch.Tensor = None, sDL: torch.Tensor = None,
+                     E_ref: float = 0.0, bulk: bool = False) -> torch.Tensor:
+    """Sigma(E) [B, nc, nc] of one lead at real energies ``energies`` [B] (relative to ``E_ref``),
+    differentiable w.r.t. H, H_01, S, S_01, H_DL and S_DL (2-D CUDA tensors).
+
+    The same quantity as ``surface_green.selfEnergy`` (negf/surface_green.py:9-91:
+    decimation at z = E + E_ref + i eta, Sigma = (E S_DL - H_DL) g_s[:b,:b]
+    (E S_DL^H - H_DL^H) with E = energy + E_ref, or the bulk forms without H_DL),
+    for every energy in one decimation launch.  Its gradient goes through the
+    converged surface Green's function by implicit differentiation, so
+    tight-binding parameters of the leads can be fitted together with the
+    device's: pass the result as ``left_se`` / ``right_se`` to ``transmission``
+    or ``transmission_dos``.  Raises as ``selfEnergy`` does when the decimation
+    fails its residual check."""
+    e = torch.as_tensor(energies, dtype=torch.float64).reshape(-1).to(torch.complex128)
+    return _LeadSelfEnergyFn.apply(e, float(eta), float(E_ref), bool(bulk), hL, hLL, sL, sLL, hDL, sDL)
+
+
 def current(T: torch.Tensor, energy: torch.Tensor, f_left: torch.Tensor, f_right: torch.Tensor) -> torch.Tensor:
     """Landauer current sum(E) (f_L - f_R) T by Simpson's rule (no 2e/h prefactor, as the reference)."""
     e = torch.as_tensor(energy, dtype=torch.float64, device=T.device).real

@@ -271,3 +271,83 @@ def test_mixed_density_gradient_close_to_fp64():
     for k in ("hd", "hu", "hl", "sd", "su", "sl"):
         for q in range(len(g64[k])):
             assert _rel(gmx[k][q], g64[k][q].cpu().numpy()) < 1e-3, (k, q)
+
+
+def _lead(n, nc, seed):
+    rng = np.random.default_rng(seed)
+    c = lambda shape, s: torch.as_tensor(rng.normal(size=shape) * s + 1j * rng.normal(size=shape) * s)
+    h = c((n, n), 0.3)
+    hL = (h + h.mH) / 2 + torch.diag(torch.linspace(-1, 1, n)).to(torch.complex128)
+    s = c((n, n), 0.02)
+    sL = torch.eye(n, dtype=torch.complex128) + (s + s.mH) / 2
+    return [x.cuda() for x in (hL, c((n, n), 0.5), sL, c((n, n), 0.02), c((nc, n), 0.5), c((nc, n), 0.02))]
+
+
+def test_lead_self_energy_gradient_matches_finite_differences():
+    """dL/d(H, H01, S, S01, H_DL, S_DL) of a lead through the decimation fixed point (implicit
+    adjoint) against central differences of the CUDA decimation; Sigma itself against the oracle."""
+    from oracle import lead_oracle
+    from dpnegf_b200.adjoint import lead_self_energy
+    n, nc = 6, 5
+    base = _lead(n, nc, seed=3)
+    E = torch.tensor([-0.7, 0.2, 0.9], dtype=torch.float64)
+    eta = 1e-3
+    rng = np.random.default_rng(4)
+    W = torch.as_tensor(rng.normal(size=(3, nc, nc)) + 1j * rng.normal(size=(3, nc, nc))).cuda()
+
+    def loss(bl):
+        sig = lead_self_energy(*bl[:4], E, eta, hDL=bl[4], sDL=bl[5])
+        return (W * sig).sum().real, sig
+
+    leaves = [x.clone().requires_grad_(True) for x in base]
+    L0, sig = loss(leaves)
+    for e in range(3):
+        ref = lead_oracle.self_energy(*(x.cpu().numpy() for x in base[:4]), float(E[e]),
+                                      base[4].cpu().numpy(), base[5].cpu().numpy(), etaLead=eta)[0]
+        assert _rel(sig[e], ref) < 1e-9
+    L0.backward()
+    h = 1e-6
+    with torch.no_grad():
+        for k in range(6):
+            X = leaves[k]
+            for _ in range(2):
+                i, j = rng.integers(X.shape[0]), rng.integers(X.shape[1])
+                for part, unit in (("re", 1.0), ("im", 1j)):
+                    def shifted(sgn):
+                        bl = [x.clone() for x in base]
+                        bl[k][i, j] += sgn * h * unit
+                        return loss(bl)[0].item()
+                    fd = (shifted(1) - shifted(-1)) / (2 * h)
+                    ad = X.grad[i, j].real.item() if part == "re" else X.grad[i, j].imag.item()
+                    assert abs(fd - ad) <= 1e-5 * max(1.0, abs(ad)), (k, i, j, part, fd, ad)
+
+
+def test_transmission_gradient_reaches_lead_blocks():
+    """T(E) with Sigma_L from lead_self_energy: d(sum T)/d(lead H01) by autograd (device adjoint ->
+    dT/dSigma -> decimation adjoint) against central differences."""
+    from dpnegf_b200 import workload
+    from dpnegf_b200.adjoint import lead_self_energy, transmission
+    n = 8
+    hL, hLL, sL, sLL, hDL, sDL = _lead(n, n, seed=7)
+    dims = [n, 10, n]
+    dev = workload.random_device(0, 0, seed=8, block_dims=dims)
+    blocks = [[x.cuda() for x in getattr(dev, k)] for k in ("hd", "hu", "hl", "sd", "su", "sl")]
+    E = torch.tensor([-0.5, 0.3], dtype=torch.float64)
+    seR = workload.random_self_energy(2, n, seed=9).cuda()
+
+    def total(h01):
+        sigL = lead_self_energy(hL, h01, sL, sLL, E, 1e-3, hDL=hDL, sDL=sDL)
+        T = transmission(*blocks, E.to(torch.complex128).cuda(), sigL, seR, eta=1e-5)
+        return T.sum()
+
+    h01 = hLL.clone().requires_grad_(True)
+    total(h01).backward()
+    h = 1e-6
+    with torch.no_grad():
+        for (i, j) in ((0, 1), (3, 5)):
+            for part, unit in (("re", 1.0), ("im", 1j)):
+                d = torch.zeros_like(hLL)
+                d[i, j] = h * unit
+                fd = (total(hLL + d) - total(hLL - d)).item() / (2 * h)
+                ad = h01.grad[i, j].real.item() if part == "re" else h01.grad[i, j].imag.item()
+                assert abs(fd - ad) <= 1e-5 * max(1.0, abs(ad)), (i, j, part, fd, ad)

@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--phases", action="store_true", help="report per-phase SM-cycle shares")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision and adjoint legs")
     ap.add_argument("--refine-steps", type=int, default=3)
+    ap.add_argument("--inverse", default=None, choices=["gj", "block"],
+                    help="Schur-complement inverse: pivoted Gauss-Jordan or recursive 2x2 blocks "
+                         "(default: the autotuned scheme, else block)")
     ap.add_argument("--torch-energies", type=int, default=128,
                     help="energies of the torch-on-CUDA reference-path sample (0: skip that leg)")
     return ap.parse_args()
@@ -400,7 +403,7 @@ def main():
 
     def step(s, ev=None, phase=False):
         return rgf_plan.run(geoms[s], [Ed], [seL], [seR], eta=args.eta, outputs=(), trans=True, dos=True,
-                            check=False, events=ev, phase=phase)
+                            check=False, events=ev, phase=phase, inverse=args.inverse)
 
     for s in range(args.warmup):
         r = step(s)
@@ -447,7 +450,7 @@ def main():
         phases = {}
         for prec in ("fp64", "mixed"):
             r = rgf_plan.run(geoms[args.warmup], [Ed], [seL], [seR], eta=args.eta, outputs=(), trans=True,
-                             dos=True, check=False, phase=True, precision=prec)
+                             dos=True, check=False, phase=True, precision=prec, inverse=args.inverse)
             torch.cuda.synchronize()
             pc = r.phase_cycles.sum(0).double()
             phases[prec] = {n: float(v) for n, v in zip(_lib.PHASES, (pc / pc.sum()).tolist()) if v > 0}

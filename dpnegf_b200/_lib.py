@@ -112,6 +112,8 @@ class NegfRgfProblem(ctypes.Structure):
         ("refine_steps", ctypes.c_int32),
         ("inv_ob", ctypes.c_int32),
         ("s_out", ctypes.c_void_p),
+        ("inv_mode", ctypes.c_int32),
+        ("pad1", ctypes.c_int32),
     ]
 
 

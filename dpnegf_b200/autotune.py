@@ -1,12 +1,17 @@
 """Autotuner for the sweep's schedule knobs.
 
-The knob tuned here is the Gauss-Jordan outer block width ``inv_ob`` of the
-in-kernel inverse (64, 128, 256 or 512 columns; 32 is accepted too but never
-won).  Narrower outer blocks move work from the panels' rank-32 updates (FP64
-tensor cores, fed from shared memory) to the outer block GEMM, which runs on
-the tile GEMM, or on the tcgen05 3xTF32 GEMM in the mixed sweep; a width of at
-least n leaves no outer update.  Which split is fastest depends on block size
-and precision.  Results agree to rounding for every width.
+Two knobs of the in-kernel Schur-complement inverse are tuned together: the
+inverse scheme (``inverse``: "block", recursive 2x2 blocks with every update on
+the tile GEMM and pivoted Gauss-Jordan only on 64-wide leaves, or "gj", pivoted
+Gauss-Jordan over the whole block) and the Gauss-Jordan outer block width
+``inv_ob`` (64, 128, 256 or 512 columns; 32 is accepted too but never won),
+which "gj" uses throughout and "block" uses when its residual probe sends an
+item back to Gauss-Jordan.  Narrower outer blocks move work from the panels'
+rank-32 updates (FP64 tensor cores, fed from shared memory) to the outer block
+GEMM, which runs on the tile GEMM, or on the tcgen05 3xTF32 GEMM in the mixed
+sweep; a width of at least n leaves no outer update.  Which choice is fastest
+depends on block size and precision.  Results agree to rounding for every
+choice.
 
 ``tune(n, precision)`` times each candidate on a short synthetic sweep of
 block size ``n`` (one item per SM, four blocks) and stores the winner per
@@ -21,7 +26,7 @@ import json
 import os
 from typing import Callable, Dict, Optional
 
-CANDIDATES = {"inv_ob": (64, 128, 256, 512)}
+CANDIDATES = {"inv_ob": (64, 128, 256, 512), "inverse": ("block", "gj")}
 BUCKETS = (32, 64, 96, 128, 192, 256, 384, 512)
 SHIPPED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "autotune_b200.json")
 _loaded: Dict[str, dict] = {}
@@ -85,7 +90,7 @@ def store(n: int, precision: str, best: dict, times: dict, path: Optional[str] =
     _loaded[path] = table
 
 
-def _time_sweep(n: int, precision: str, inv_ob: int, L: int = 4, repeats: int = 2) -> float:
+def _time_sweep(n: int, precision: str, inv_ob: int, inverse: str = "gj", L: int = 4, repeats: int = 2) -> float:
     """Device time (ms) of one sweep (T + DOS) of a synthetic device, one item per SM."""
     import torch
     from . import _lib, rgf_plan, workload
@@ -97,7 +102,7 @@ def _time_sweep(n: int, precision: str, inv_ob: int, L: int = 4, repeats: int = 
     seR = workload.random_self_energy(B, n, seed=13).cuda()
     E = workload.energy_grid(B).to(torch.complex128).cuda()
     ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-    kw = dict(eta=1e-5, outputs=(), trans=True, dos=True, precision=precision, inv_ob=inv_ob)
+    kw = dict(eta=1e-5, outputs=(), trans=True, dos=True, precision=precision, inv_ob=inv_ob, inverse=inverse)
     rgf_plan.run(geom, [E], [seL], [seR], **kw)
     best = float("inf")
     for _ in range(repeats):
@@ -108,12 +113,16 @@ def _time_sweep(n: int, precision: str, inv_ob: int, L: int = 4, repeats: int = 
 
 
 def tune(n: int, precision: str = "fp64", write: bool = True, path: Optional[str] = None,
-         timer: Optional[Callable[[int, str, int], float]] = None) -> dict:
-    """Time every inv_ob candidate for block size n and keep the fastest."""
+         timer: Optional[Callable[..., float]] = None) -> dict:
+    """Time every Gauss-Jordan inv_ob candidate and the block inverse for block size n and keep
+    the fastest scheme, with the fastest Gauss-Jordan width (the block scheme's fallback)."""
     timer = timer or _time_sweep
     cands = [ob for ob in CANDIDATES["inv_ob"] if ob < 2 * n] or [CANDIDATES["inv_ob"][0]]
-    times = {str(ob): float(timer(n, precision, ob)) for ob in cands}
-    best = {"inv_ob": int(min(times, key=lambda k: times[k]))}
+    times = {str(ob): float(timer(n, precision, ob, inverse="gj")) for ob in cands}
+    ob_best = int(min(times, key=lambda k: times[k]))
+    times["block"] = float(timer(n, precision, ob_best, inverse="block"))
+    scheme = "block" if times["block"] < times[str(ob_best)] else "gj"
+    best = {"inverse": scheme, "inv_ob": ob_best}
     if write:
         store(n, precision, best, times, path=path)
     return best

@@ -210,6 +210,99 @@ NEGF_DEV void gemm_epi(const GemmArgs& g, cplx* smem, const Epi& e) {
   else cta_gemm_epi<OPA, OPB, true>(g, smem, e);
 }
 
+// Recursive 2x2 block inverse (inv_mode 1): G = W^-1, W destroyed.  With
+// W = [[A11, A12], [A21, A22]] split at h:
+//   X = A11^-1,  U = A21 X,  S = A22 - U A12,  Y = S^-1,  T = X A12,
+//   G = [[X + T Y U, -T Y], [-Y U, Y]]
+// X and Y recursively down to INVB_LEAF-wide leaves, which the pivoted
+// Gauss-Jordan inverse handles; every other operation is a CTA GEMM, in place
+// in W and G (U in G21, S in W22, T in W11 once A11 is consumed, -Y U via W21).
+// Pivoting stays inside the leaves, so the leading blocks must be nonsingular:
+// true for the retarded problem with eta > 0, whose matrices have a
+// positive-definite imaginary part (so have all their leading blocks and
+// Schur complements).  Work n^3 complex MACs, as for Gauss-Jordan.
+constexpr int INVB_LEAF = 64;
+template <int LV, bool MX>
+__device__ __noinline__ int cta_inverse_blk(cplx* W, int64_t ldw, int n, cplx* G, int64_t ldg, cplx* smem,
+                                           PhaseClock& pc, cplx* snap) {
+  if constexpr (LV == 0) {
+    return cta_inverse<true, MX>(W, ldw, n, G, ldg, reinterpret_cast<char*>(smem), &pc, snap, INV_OB_MAX);
+  } else {
+    if (n <= INVB_LEAF)
+      return cta_inverse<true, MX>(W, ldw, n, G, ldg, reinterpret_cast<char*>(smem), &pc, snap, INV_OB_MAX);
+    const int h = ((n + 1) / 2 + 7) & ~7, m = n - h;
+    cplx *W11 = W, *W12 = W + h, *W21 = W + (int64_t)h * ldw, *W22 = W21 + h;
+    cplx *G11 = G, *G12 = G + h, *G21 = G + (int64_t)h * ldg, *G22 = G21 + h;
+    const cplx ONE = cmk(1.0, 0.0), MONE = cmk(-1.0, 0.0);
+    int bad = cta_inverse_blk<LV - 1, MX>(W11, ldw, h, G11, ldg, smem, pc, snap);             // X
+    gemm<OP_N, OP_N, MX>(smem, m, h, h, W21, ldw, G11, ldg, G21, ldg);                         // U = A21 X
+    gemm<OP_N, OP_N, MX>(smem, m, m, h, G21, ldg, W12, ldw, W22, ldw, MONE, W22, ldw);         // S
+    pc.mark(PH_INV_UPDATE);
+    bad |= cta_inverse_blk<LV - 1, MX>(W22, ldw, m, G22, ldg, smem, pc, snap);               // Y
+    gemm<OP_N, OP_N, MX>(smem, h, m, h, G11, ldg, W12, ldw, W11, ldw);                         // T = X A12
+    gemm<OP_N, OP_N, MX>(smem, h, m, m, W11, ldw, G22, ldg, G12, ldg, MONE);                  // G12 = -T Y
+    gemm<OP_N, OP_N, MX>(smem, h, h, m, G12, ldg, G21, ldg, G11, ldg, MONE, G11, ldg);       // X + T Y U
+    gemm<OP_N, OP_N, MX>(smem, m, h, m, G22, ldg, G21, ldg, W21, ldw, MONE);                  // -Y U
+    for (int e = threadIdx.x; e < m * h; e += CTA_THREADS) {
+      const int i = e / h, j = e % h;
+      G21[(int64_t)i * ldg + j] = W21[(int64_t)i * ldw + j];
+    }
+    __syncthreads();
+    pc.mark(PH_INV_UPDATE);
+    (void)ONE;
+    return bad;
+  }
+}
+
+// Residual probe of an inverse G of A (n x n, row stride n): with a fixed
+// sign vector v (entries +-1 +-i from a hash of the index), y = G v and
+// r = A y - v; true when max|r| <= tol n max|A| max|y| (a backward-stable
+// inverse leaves about n u there) and everything is finite.  Whole CTA (the
+// verdict is uniform); y lives in smem.
+NEGF_DEV bool inv_probe(const cplx* A, const cplx* G, int n, double tol, cplx* smem, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  auto v = [](int j) {
+    const unsigned h = (unsigned)(j + 1) * 2654435761u;
+    return cmk((h & 0x10000u) ? 1.0 : -1.0, (h & 0x20000u) ? 1.0 : -1.0);
+  };
+  cplx* y = smem;
+  for (int i = warp; i < n; i += CTA_THREADS / 32) {
+    cplx acc = cmk(0.0, 0.0);
+    for (int j = lane; j < n; j += 32) acc = cfma(G[(int64_t)i * n + j], v(j), acc);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
+    }
+    if (lane == 0) y[i] = acc;
+  }
+  __syncthreads();
+  double rmax = 0.0, amax = 0.0, ymax = 0.0;
+  for (int i = warp; i < n; i += CTA_THREADS / 32) {
+    cplx acc = cmk(0.0, 0.0);
+    double am = 0.0;
+    for (int j = lane; j < n; j += 32) {
+      const cplx a = A[(int64_t)i * n + j];
+      acc = cfma(a, y[j], acc);
+      am = fmax(am, cabs1(a));
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
+      am = fmax(am, __shfl_xor_sync(0xffffffffu, am, off));
+    }
+    const double r = cabs1(csub(acc, v(i)));
+    rmax = (r == r) ? fmax(rmax, r) : INFINITY;
+    amax = fmax(amax, am);
+    ymax = fmax(ymax, cabs1(y[i]));
+  }
+  rmax = cta_max(rmax, red);
+  amax = cta_max(amax, red);
+  ymax = cta_max(ymax, red);
+  return rmax <= tol * (double)n * amax * ymax;
+}
+
 // Adjoint epilogue: W (rows of block q x cols of block p) contributes
 // dL/dX_pq = 2c W^H to the H accumulator and -2c conj(z) W^H to the S one
 // (X = H + Sigma - zS); the lead corners of the edge blocks also feed the
@@ -343,8 +436,21 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
       __syncthreads();
       pc.mark(PH_FORM);
     }
-    bad |= cta_inverse<true, MX>(sb.W, nq, nq, gptr(q), nq, smem_raw, &pc, sb.tE,  // tE: pivot-row snapshot
-                                 P.inv_ob > 0 ? P.inv_ob : INV_OB);
+    bool gj = P.inv_mode != 1;
+    if (!gj) {
+      // block inverse on a copy of W; a failed residual probe (or a singular leaf) falls
+      // back to the pivoted Gauss-Jordan on the saved W
+      copy_mat(sb.tD, sb.W, nq, nq, smem);
+      const int bb = cta_inverse_blk<3, MX>(sb.W, nq, nq, gptr(q), nq, smem, pc, sb.tE);
+      if (bb || !inv_probe(sb.tD, gptr(q), nq, MX ? 1e-4 : 1e-10, smem, red)) {
+        copy_mat(sb.W, sb.tD, nq, nq, smem);
+        gj = true;
+      }
+      pc.mark(PH_INV_GATHER);
+    }
+    if (gj)
+      bad |= cta_inverse<true, MX>(sb.W, nq, nq, gptr(q), nq, smem_raw, &pc, sb.tE,  // tE: pivot-row snapshot
+                                   P.inv_ob > 0 ? P.inv_ob : INV_OB);
     if (dosg) {
       // dg_q/dz = -g_q Kd g_q with Kd = S_q - (L dg_{q-1} - sl g_{q-1}) U + (L g_{q-1}) su
       // (d/dz of g_q^-1 = zS_q - H_q - Sigma - L g U, dL/dz = -sl, dU/dz = -su; sb.T1 = L g_{q-1})
@@ -878,6 +984,7 @@ int negf_rgf_run(const NegfRgfProblem* p, void* stream) {
     return NEGF_ERR_ARGUMENT;
   if ((p->flags & NEGF_REFINE) && (p->col_slab <= 0 || !(p->flags & NEGF_TRANS))) return NEGF_ERR_ARGUMENT;
   if ((p->flags & NEGF_ADJ_DOS) && !(p->flags & NEGF_ADJOINT)) return NEGF_ERR_ARGUMENT;
+  if (p->inv_mode != 0 && p->inv_mode != 1) return NEGF_ERR_ARGUMENT;
   if (p->inv_ob != 0 && p->inv_ob != 32 && p->inv_ob != 64 && p->inv_ob != 128 && p->inv_ob != 256 &&
       p->inv_ob != 512)
     return NEGF_ERR_ARGUMENT;

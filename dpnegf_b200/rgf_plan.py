@@ -209,7 +209,7 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
         s_in: Optional[List[List[Optional[torch.Tensor]]]] = None,
         s_out: Optional[List[List[Optional[torch.Tensor]]]] = None,
         n_slots=None, check=True, stream=None, phase=False, events=None, adjoint_w=None, adjoint_w_dos=None,
-        precision="fp64", refine=False, refine_steps=1, defer=False, inv_ob=None):
+        precision="fp64", refine=False, refine_steps=1, defer=False, inv_ob=None, inverse=None):
     """Run the batched sweep.
 
     ``energies[d]`` is a 1-D tensor of B_d energies for device d; ``se_l[d]``
@@ -230,6 +230,16 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     (FP32-accurate products; pivoting, panels and storage stay FP64);
     ``refine=True`` (with ``trans``) adds ``refine_steps`` FP64-residual
     refinement steps of the column G_{:,N} that T(E) is read from.
+    ``inverse="block"`` inverts each Schur complement by recursive
+    2x2 blocks (pivoted Gauss-Jordan only on 64-wide leaves, all updates on
+    the block GEMM), which needs nonsingular leading sub-blocks: eta > 0
+    guarantees them for Hermitian H, positive-definite S and retarded
+    self-energies.  Every block inverse is checked by a residual probe and
+    an item whose check fails is redone with the pivoted Gauss-Jordan
+    inverse, so other inputs (eta = 0, arbitrary matrices) stay exact.
+    ``inverse="gj"`` uses the pivoted Gauss-Jordan inverse throughout; by
+    default the autotuned scheme for this GPU, block size and precision, else
+    "block".
     ``inv_ob`` is the inverse's outer block width (32..512); by default the
     autotuned value for this GPU, block size and precision (``autotune.lookup``),
     else 128.
@@ -442,10 +452,17 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     if refine or adjoint:
         prob.col_slab = max(int(geom.col_slab), 1)
     prob.refine_steps = int(refine_steps)
-    if inv_ob is None:
+    if inv_ob is None or inverse is None:
         from . import autotune
-        inv_ob = autotune.lookup(geom.max_n, precision).get("inv_ob", 0)
+        tuned = autotune.lookup(geom.max_n, precision)
+        if inv_ob is None:
+            inv_ob = tuned.get("inv_ob", 0)
+        if inverse is None:
+            inverse = tuned.get("inverse", "block")
     prob.inv_ob = int(inv_ob)
+    if inverse not in ("gj", "block"):
+        raise ValueError(f"inverse must be 'gj' or 'block', not {inverse!r}")
+    prob.inv_mode = 1 if inverse == "block" else 0
     need = lib.negf_rgf_scratch_bytes(ctypes.byref(prob))
     scratch = torch.empty(max(need, 256), dtype=torch.uint8, device=dev)
     prob.scratch = scratch.data_ptr()

@@ -157,6 +157,13 @@ typedef struct NegfRgfProblem {
   int32_t inv_ob;           /* Gauss-Jordan outer block width: 32, 64, 128, 256 or 512 columns (0 = 128);
                                results agree to rounding, the speed depends on block size and precision */
   const double* s_out;      /* complex128 arena of Sigma^out blocks (NEGF_GREATER) */
+  int32_t inv_mode;         /* 0: Gauss-Jordan with partial pivoting over the whole block (inv_ob);
+                               1: recursive 2x2 block inverse, pivoting only inside 64-wide leaves and
+                               every update a CTA GEMM.  Mode 1 needs nonsingular leading sub-blocks,
+                               which the retarded problem guarantees for eta > 0 (zS - H - Sigma - L g U
+                               has a positive-definite imaginary part when H is Hermitian, S positive
+                               definite and Im Sigma <= 0) */
+  int32_t pad1;
 } NegfRgfProblem;
 
 /* ---- Lopez-Sancho lead decimation ------------------------------------ */

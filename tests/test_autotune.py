@@ -21,9 +21,12 @@ def test_tune_store_lookup(tmp_path, monkeypatch):
     assert autotune.lookup(250, "fp64") == {"inv_ob": 128}          # shipped table
     assert autotune.lookup(250, "mixed") == {}                       # untuned
     times = {64: 1.0, 128: 2.0, 256: 3.0, 512: 0.5}
-    best = autotune.tune(250, "fp64", timer=lambda n, p, ob: times[ob])
-    assert best == {"inv_ob": 64}  # 512 >= 2n is not a distinct candidate
-    assert autotune.lookup(250, "fp64") == {"inv_ob": 64}           # user cache wins
+    timer = lambda n, p, ob, inverse: times[ob] if inverse == "gj" else 0.8
+    best = autotune.tune(250, "fp64", timer=timer)
+    assert best == {"inverse": "block", "inv_ob": 64}  # 512 >= 2n is not a distinct candidate
+    assert autotune.lookup(250, "fp64") == {"inverse": "block", "inv_ob": 64}  # user cache wins
     saved = json.loads(user.read_text())
-    assert saved["FakeGPU|fp64|n<=256"]["ms"] == {"64": 1.0, "128": 2.0, "256": 3.0}
+    assert saved["FakeGPU|fp64|n<=256"]["ms"] == {"64": 1.0, "128": 2.0, "256": 3.0, "block": 0.8}
+    slow = lambda n, p, ob, inverse: times[ob] if inverse == "gj" else 9.0
+    assert autotune.tune(100, "mixed", timer=slow) == {"inverse": "gj", "inv_ob": 64}
     autotune._loaded.clear()

@@ -134,5 +134,5 @@ def test_mixed_outer_block_widths(inv_ob):
     dims = [200, 136, 200]
     dev, seL, seR, E = _case(dims, 3, seed=51)
     _, T, _ = _oracle(dev, seL, seR, E)
-    r = _run(dev, seL, seR, E, outputs=(), trans=True, precision="mixed", refine=True, inv_ob=inv_ob)
+    r = _run(dev, seL, seR, E, outputs=(), trans=True, precision="mixed", refine=True, inv_ob=inv_ob, inverse="gj")
     assert np.abs(r.trans.cpu().numpy() - T).max() < T_ATOL

@@ -207,7 +207,7 @@ def test_inverse_outer_block_widths_agree(inv_ob):
     dev, seL, seR, E, _ = _oracle_case(dims, 2, seed=29)
     geom = rgf_plan.Geometry([rgf_plan.DeviceBlocks(dev.hd, dev.hu, dev.hl, dev.sd, dev.su, dev.sl)])
     res = rgf_plan.run(geom, [E.cuda()], [seL.cuda()], [seR.cuda()], eta=1e-5, outputs=("grd", "g_trans"),
-                       inv_ob=inv_ob)
+                       inv_ob=inv_ob, inverse="gj")
     ref = rgf_oracle.rgf(E.numpy(), [x.numpy() for x in dev.hl], [x.numpy() for x in dev.hd],
                          [x.numpy() for x in dev.hu], [x.numpy() for x in dev.sd],
                          [x.numpy() for x in dev.su], [x.numpy() for x in dev.sl],
@@ -215,3 +215,34 @@ def test_inverse_outer_block_widths_agree(inv_ob):
     for q, w in enumerate(ref["grd"]):
         _assert_block_close(res.blocks[0]["grd"][q], w, f"grd[{q}] ob={inv_ob}")
     _assert_block_close(res.blocks[0]["g_trans"], ref["g_trans"], f"g_trans ob={inv_ob}")
+
+
+@pytest.mark.parametrize("dims,B", [([64] * 4, 3), ([70, 33, 128, 65], 2), ([256] * 3, 2), ([300, 280], 1),
+                                     ([17], 3), ([512, 96], 1)])
+def test_block_inverse_matches_oracle(dims, B):
+    """inverse="block" (recursive 2x2 blocks, pivoted 64-wide leaves) gives the oracle's blocks
+    to 1e-10: ragged splits, a single leaf, three recursion levels (n = 512)."""
+    from dpnegf_b200 import rgf_plan
+    dev, seL, seR, E, _ = _oracle_case(dims, B, seed=len(dims) * 5 + dims[0])
+    geom = rgf_plan.Geometry([rgf_plan.DeviceBlocks(dev.hd, dev.hu, dev.hl, dev.sd, dev.su, dev.sl)])
+    res = rgf_plan.run(geom, [E.cuda()], [seL.cuda()], [seR.cuda()], eta=1e-5,
+                       outputs=("g_trans", "grd", "grl", "gru"), trans=True, dos=True, inverse="block")
+    ref = rgf_oracle.rgf(E.numpy(), [x.numpy() for x in dev.hl], [x.numpy() for x in dev.hd],
+                         [x.numpy() for x in dev.hu], [x.numpy() for x in dev.sd],
+                         [x.numpy() for x in dev.su], [x.numpy() for x in dev.sl],
+                         seL.numpy(), seR.numpy(), eta=1e-5)
+    blocks = res.blocks[0]
+    for tag in ("g_trans", "grd", "grl", "gru"):
+        want = ref[tag]
+        if isinstance(want, list):
+            for q, (g, w) in enumerate(zip(blocks[tag], want)):
+                _assert_block_close(g, w, f"{tag}[{q}]")
+        else:
+            _assert_block_close(blocks[tag], want, tag)
+    sd = [x.numpy() for x in dev.sd]
+    T_ref = rgf_oracle.transmission(ref["g_trans"], rgf_oracle.gamma_from_se(seL.numpy()),
+                                    rgf_oracle.gamma_from_se(seR.numpy()))
+    D_ref = rgf_oracle.dos(ref["grd"], ref["grl"], ref["gru"], sd, [x.numpy() for x in dev.su],
+                           [x.numpy() for x in dev.sl])
+    np.testing.assert_allclose(res.trans.cpu().numpy(), T_ref, rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(res.dos.cpu().numpy(), D_ref, rtol=1e-10, atol=1e-12)

@@ -6,9 +6,14 @@ Same constructor, attributes and methods as the reference ``LeadProperty``
 computed by the batched Lopez-Sancho kernel; ``energy`` may also be a 1-D
 tensor of energies, in which case ``self.se`` is ``[B, n, n]`` from a single
 launch (the reference computes one energy per call and stacks them in the
-runner, runner/NEGF.py:762-778).  Saved self-energies are read back in the
-``pth`` format; the HDF5 cache and the joblib pool of the reference are not
-part of this package.
+runner, runner/NEGF.py:762-778).  Saved self-energies are found and read as
+the reference does (``_get_save_path`` / ``_load_self_energy``: per-(k, E)
+``pth`` files, or the per-lead HDF5 files with groups ``E_{e:.8f}`` and
+datasets ``k_{k0}_{k1}_{k2}``, the HDF5 form when h5py is importable).
+``compute_all_self_energy`` replaces the reference's joblib pool over (k, E)
+(negf/lead_property.py:599-683) with one decimation launch per (lead, k) over
+the whole energy grid; it returns the self-energies in memory for the sweep
+and writes the same files.
 """
 import logging
 import os
@@ -57,18 +62,55 @@ class LeadProperty(object):
 
     # ------------------------------------------------------------------ API
     def self_energy(self, kpoint, energy, eta_lead: float = 1e-5, method: str = "Lopez-Sancho",
-                    save_path: str = None, save_format: str = "pth", se_info_display: bool = False,
+                    save_path: str = None, save_format: str = "h5", se_info_display: bool = False,
                     HS_inmem: bool = True):
-        """Set ``self.se`` for ``kpoint`` at ``energy`` (scalar or [B], relative to E_ref)."""
+        """Set ``self.se`` for ``kpoint`` at ``energy`` (scalar or [B], relative to E_ref): loaded
+        from a saved file when one exists at the reference's path (lead_property.py:105-158, a
+        scalar energy), else computed on the GPU."""
         assert len(np.array(kpoint).reshape(-1)) == 3
         if not isinstance(energy, torch.Tensor):
             energy = torch.tensor(energy)
-        if save_path is not None and save_format == "pth" and os.path.isfile(save_path):
-            if se_info_display:
-                log.info(f"Loading {self.tab} self-energy from {save_path}")
-            self.se = torch.load(save_path, weights_only=False)
-            return
+        if energy.ndim == 0:
+            path = self._get_save_path(kpoint, energy, save_format, save_path)
+            if os.path.isfile(path):
+                if se_info_display:
+                    log.info(f"Loading {self.tab} self-energy from {path}")
+                self.se = self._load_self_energy(path, kpoint, energy, save_format)
+                return
         self.se = self.self_energy_cal(kpoint, energy, eta_lead=eta_lead, method=method, HS_inmem=HS_inmem)
+
+    def _get_save_path(self, kpoint, energy, save_format: str, save_path: str = None):
+        """File of a saved self-energy, named as the reference names it (lead_property.py:160-218)."""
+        kx, ky, kz = np.asarray(kpoint, dtype=float).reshape(3)
+        ev = energy.item() if hasattr(energy, "item") else float(energy)
+        if save_format not in ("pth", "h5"):
+            raise ValueError(f"Unsupported save_format {save_format}, only 'pth' and 'h5' are supported.")
+        if save_path is not None and not os.path.isdir(save_path):
+            return save_path
+        parent = save_path if save_path is not None else os.path.join(self.results_path or "", "self_energy")
+        if save_format == "pth":
+            return os.path.join(parent, f"se_{self.tab}_k{kx:.4f}_{ky:.4f}_{kz:.4f}_E{ev:.6f}.pth")
+        if self.tab not in ("lead_L", "lead_R"):
+            raise ValueError(f"Unsupported tab {self.tab} for h5 save.")
+        return os.path.join(parent, "self_energy_leadL.h5" if self.tab == "lead_L" else "self_energy_leadR.h5")
+
+    @staticmethod
+    def _load_self_energy(save_path: str, kpoint, energy, save_format: str):
+        """Read a saved self-energy (lead_property.py:220-264)."""
+        if save_format == "pth":
+            try:
+                return torch.load(save_path, weights_only=False)
+            except Exception as e:
+                raise IOError(f"Failed to load self-energy from {save_path} (pth format).") from e
+        if save_format == "h5":
+            ev = energy.item() if hasattr(energy, "item") else float(energy)
+            try:
+                return torch.as_tensor(read_from_hdf5(save_path, kpoint, ev), dtype=torch.complex128)
+            except KeyError as e:
+                kx, ky, kz = np.asarray(kpoint, dtype=float).reshape(3)
+                raise KeyError(f"Cannot find self-energy in {save_path} for k=({kx:.4f},{ky:.4f},{kz:.4f}), "
+                               f"E={ev:.6f}") from e
+        raise ValueError(f"Unsupported save_format {save_format}, only 'pth' and 'h5' are supported.")
 
     def self_energy_cal(self, kpoint, energy, eta_lead: float = 1e-5, method: str = "Lopez-Sancho",
                         se_numba_jit=None, HS_inmem: bool = True):
@@ -170,3 +212,85 @@ class LeadProperty(object):
     @property
     def gamma(self):
         return self.sigmaLR2Gamma(self.se)
+
+
+def _h5py():
+    try:
+        import h5py
+    except ImportError as e:
+        raise ImportError("the HDF5 self-energy files need h5py (not installed); use save_format='pth'") from e
+    return h5py
+
+
+def hdf5_keys(k, e):
+    """Group and dataset name of the self-energy at (k, e) in the per-lead HDF5 files
+    (negf/lead_property.py:932-952)."""
+    return f"E_{e:.8f}", f"k_{k[0]}_{k[1]}_{k[2]}"
+
+
+def write_to_hdf5(h5_path, k, e, se):
+    h5py = _h5py()
+    g, d = hdf5_keys(k, e)
+    with h5py.File(h5_path, "a") as f:
+        grp = f.require_group(g)
+        if d not in grp:
+            grp.create_dataset(d, data=torch.as_tensor(se).cpu().numpy(), compression="gzip")
+
+
+def read_from_hdf5(h5_path, k, e):
+    h5py = _h5py()
+    g, d = hdf5_keys(k, e)
+    with h5py.File(h5_path, "r") as f:
+        if g in f and d in f[g]:
+            return f[g][d][:]
+    raise KeyError(f"Data for kpoint {k} and energy {e} not found.")
+
+
+def compute_all_self_energy(eta, lead_L, lead_R, kpoints_grid, energy_grid, self_energy_save_path=None,
+                            n_jobs=-1, batch_size=200, n_cpus=None, se_numba_jit=None, save_format="h5"):
+    """Self-energies of both leads at every (k, E) (negf/lead_property.py:599-683).
+
+    The reference spreads the (k, E) pairs over a joblib process pool and merges
+    per-task HDF5 files; here every (lead, k) is one Lopez-Sancho launch over the
+    whole energy grid on the GPU (Bloch-unfolded leads included), and the results
+    come back in memory as ``{"lead_L": {k: [B, n, n]}, "lead_R": {...}}`` (k as a
+    tuple of floats, rows in ``energy_grid`` order) for the sweep to use directly.
+    They are also written where the reference writes them: ``save_format="h5"``
+    (default, needs h5py) gives ``self_energy_leadL.h5`` / ``self_energy_leadR.h5``
+    with groups ``E_{e:.8f}`` and datasets ``k_{k0}_{k1}_{k2}``; ``"pth"`` gives the
+    per-(k, E) files ``LeadProperty.self_energy(save_format="pth")`` reads;
+    ``None`` writes nothing.  ``n_jobs``, ``batch_size``, ``n_cpus`` and
+    ``se_numba_jit`` size the reference's process pool and are accepted for
+    compatibility only.
+    """
+    if self_energy_save_path is None:
+        if lead_L.results_path != lead_R.results_path:
+            log.warning("The results_path of lead_L and lead_R are different. "
+                        "Self energy files will be saved in lead_L's results_path.")
+        self_energy_save_path = os.path.join(lead_L.results_path, "self_energy")
+    if save_format is not None:
+        if save_format == "h5":
+            _h5py()
+        os.makedirs(self_energy_save_path, exist_ok=True)
+    energies = [float(e) for e in np.asarray(energy_grid, dtype=float).reshape(-1)]
+    E = torch.tensor(energies, dtype=torch.float64)
+    out = {"lead_L": {}, "lead_R": {}}
+    seen = []
+    for k in kpoints_grid:
+        key = tuple(float(x) for x in np.asarray(k, dtype=float).reshape(3))
+        if key in seen:
+            continue
+        seen.append(key)
+        for lead in (lead_L, lead_R):
+            se = lead.self_energy_cal(kpoint=k, energy=E, eta_lead=eta)
+            out[lead.tab][key] = se
+            if save_format == "h5":
+                path = os.path.join(self_energy_save_path,
+                                    "self_energy_leadL.h5" if lead.tab == "lead_L" else "self_energy_leadR.h5")
+                for i, e in enumerate(energies):
+                    write_to_hdf5(path, k, e, se[i])
+            elif save_format == "pth":
+                for i, e in enumerate(energies):
+                    torch.save(se[i].detach().cpu().clone(),
+                               lead._get_save_path(k, torch.tensor(e), "pth", self_energy_save_path))
+    return out

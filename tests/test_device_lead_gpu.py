@@ -172,3 +172,31 @@ def test_ozaki_equilibrium_density_matches_oracle():
                                                 lR.voltage, fL, fR, gamma_R)
     assert _rel(DM_eq, ref_eq) < 1e-9
     assert _rel(DM_neq, ref_neq) < 1e-9
+
+
+def test_compute_all_self_energy_batched_and_saved(tmp_path):
+    """compute_all_self_energy: every (lead, k) in one decimation launch over the energy grid,
+    equal to per-(k, E) selfEnergy (oracle) to 1e-9; its pth files are what
+    LeadProperty.self_energy(save_format="pth") then loads."""
+    from dpnegf_b200 import workload
+    from dpnegf_b200.lead_property import LeadProperty, compute_all_self_energy
+    dev = workload.random_device(16, 4, seed=61)
+    ham = FakeHamiltonian(dev, [1] * 64, leads={"lead_L": dev.lead_L, "lead_R": dev.lead_R})
+    leads = [LeadProperty(t, ham, None, str(tmp_path), voltage=v, efermi=0.1)
+             for t, v in (("lead_L", 0.05), ("lead_R", -0.05))]
+    ks = [[0.0, 0.0, 0.0], [0.0, 0.25, 0.0]]
+    E = [-0.8, -0.1, 0.4, 0.9]
+    out = compute_all_self_energy(1e-5, leads[0], leads[1], ks, E, save_format="pth")
+    for lp in leads:
+        L = dev.lead_L if lp.tab == "lead_L" else dev.lead_R
+        for k in ks:
+            se = out[lp.tab][tuple(k)]
+            assert se.shape == (4, 16, 16)
+            hL, hLL, hDL, sL, sLL, sDL = ham.get_hs_lead(k, lp.tab, lp.voltage)
+            for i, e in enumerate(E):
+                sig = lead_oracle.self_energy(hL.numpy(), hLL.numpy(), sL.numpy(), sLL.numpy(), e,
+                                              hDL.numpy(), sDL.numpy(), etaLead=1e-5, E_ref=0.1)[0]
+                assert _rel(se[i], sig) < 1e-9
+        fresh = LeadProperty(lp.tab, ham, None, str(tmp_path), voltage=lp.voltage, efermi=0.1)
+        fresh.self_energy(ks[1], E[2], eta_lead=1e-5, save_format="pth")
+        assert torch.equal(fresh.se.cpu(), out[lp.tab][tuple(ks[1])][2].cpu())

@@ -200,3 +200,42 @@ def test_compute_all_self_energy_batched_and_saved(tmp_path):
         fresh = LeadProperty(lp.tab, ham, None, str(tmp_path), voltage=lp.voltage, efermi=0.1)
         fresh.self_energy(ks[1], E[2], eta_lead=1e-5, save_format="pth")
         assert torch.equal(fresh.se.cpu(), out[lp.tab][tuple(ks[1])][2].cpu())
+
+
+def test_runner_nscf_loop_matches_oracle():
+    """runner.negf_compute_nscf (one lead launch per (lead, k), one fused sweep per k over all
+    energies) gives the oracle's T and DOS per energy, LDOS summing to DOS, T_avg = wk @ T_k."""
+    from dpnegf_b200 import workload
+    from dpnegf_b200.device_property import DeviceProperty
+    from dpnegf_b200.lead_property import LeadProperty
+    from dpnegf_b200.runner import negf_compute_nscf
+    n = 12
+    dev = workload.random_device(n, 4, seed=71)
+    ham = FakeHamiltonian(dev, [2] * (2 * n), leads={"lead_L": dev.lead_L, "lead_R": dev.lead_R})
+    dp = DeviceProperty(ham, None, "", e_T=300, E_ref=0.1)
+    lL = LeadProperty("lead_L", ham, None, "", voltage=0.0, efermi=0.1)
+    lR = LeadProperty("lead_R", ham, None, "", voltage=0.0, efermi=0.1)
+    dp.set_leadLR(lL, lR)
+    E = torch.linspace(-1.0, 1.0, 11, dtype=torch.float64)
+    ks, wk = [[0.0, 0.0, 0.0], [0.0, 0.5, 0.0]], [0.25, 0.75]
+    out = negf_compute_nscf(dp, ks, wk, E, eta_lead=1e-5, eta_device=1e-5, out_dos=True, out_ldos=True,
+                            out_current_nscf=True)
+    T_ref, D_ref = [], []
+    for e in E.numpy():
+        se = []
+        for tab in ("lead_L", "lead_R"):
+            hL, hLL, hDL, sL, sLL, sDL = ham.get_hs_lead([0, 0, 0], tab, 0.0)
+            se.append(lead_oracle.self_energy(hL.numpy(), hLL.numpy(), sL.numpy(), sLL.numpy(), e,
+                                              hDL.numpy(), sDL.numpy(), etaLead=1e-5, E_ref=0.1)[0])
+        npy = lambda xs: [x.numpy() for x in xs]
+        r = rgf_oracle.rgf(np.array([e]), npy(dev.hl), npy(dev.hd), npy(dev.hu), npy(dev.sd), npy(dev.su),
+                           npy(dev.sl), se[0][None], se[1][None], E_ref=0.1, eta=1e-5)
+        T_ref.append(rgf_oracle.transmission(r["g_trans"], rgf_oracle.gamma_from_se(se[0][None]),
+                                             rgf_oracle.gamma_from_se(se[1][None]))[0])
+        D_ref.append(rgf_oracle.dos(r["grd"], r["grl"], r["gru"], npy(dev.sd), npy(dev.su), npy(dev.sl))[0])
+    for k in ks:
+        assert _rel(out["T_k"][str(k)], np.array(T_ref)) < 1e-9
+        assert _rel(out["DOS"][str(k)], np.array(D_ref)) < 1e-9
+        assert _rel(out["LDOS"][str(k)].sum(-1), np.array(D_ref)) < 1e-9
+    assert _rel(out["T_avg"], np.array(T_ref)) < 1e-9
+    assert len(out["CURRENT_NSCF"]) == len(out["BIAS_POTENTIAL_NSCF"])

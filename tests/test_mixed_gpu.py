@@ -136,3 +136,19 @@ def test_mixed_outer_block_widths(inv_ob):
     _, T, _ = _oracle(dev, seL, seR, E)
     r = _run(dev, seL, seR, E, outputs=(), trans=True, precision="mixed", refine=True, inv_ob=inv_ob, inverse="gj")
     assert np.abs(r.trans.cpu().numpy() - T).max() < T_ATOL
+
+
+@pytest.mark.parametrize("inverse", ["block", "gj"])
+def test_mixed_with_each_inverse_scheme(inverse):
+    """Both Schur-complement inverses in the mixed sweep (the autotuner picks the block scheme
+    there from n = 384): refined T within 1e-6, unrefined T and DOS at FP32-product level."""
+    dims, B = [384, 128, 384], 2
+    dev, seL, seR, E = _case(dims, B, seed=77)
+    _, T, D = _oracle(dev, seL, seR, E)
+    raw = _run(dev, seL, seR, E, outputs=(), trans=True, dos=True, precision="mixed", inverse=inverse)
+    ref = _run(dev, seL, seR, E, outputs=(), trans=True, precision="mixed", refine=True, refine_steps=3,
+               inverse=inverse)
+    assert np.abs(ref.trans.cpu().numpy() - T).max() < T_ATOL
+    scale = max(np.abs(T).max(), 1.0)
+    assert np.abs(raw.trans.cpu().numpy() - T).max() < FP32_RTOL * scale
+    np.testing.assert_allclose(raw.dos.cpu().numpy(), D, rtol=FP32_RTOL, atol=FP32_RTOL * np.abs(D).max())

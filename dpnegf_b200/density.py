@@ -202,3 +202,102 @@ class Ozaki(Density):
             out.append(rec)
             orb0 += nE * n_orb
         return out
+
+
+class Fiori(Density):
+    """Free charge per atom on a real energy grid (mirror of negf/density.py:234-395).
+
+    The reference walks ``integrate_range`` one energy at a time: both lead
+    self-energies, a full ``cal_green_function``, then for every diagonal block
+    A_R = G_qN Gamma_R G_qN^H, A_L = i(G_qq - G_qq^H) - A_R,
+    G^n = A_L f_L(E + E_ref) + A_R f_R(E + E_ref) and G^p = A_L + A_R - G^n, and
+    per atom adds  w_E * (-1/pi) Tr_atom G^n  when E >= -potential_at_atom
+    (electrons) or  w_E * (1/pi) Tr_atom G^p  otherwise (holes)
+    (density.py:268-360).  Only diagonals of those blocks enter the traces, so
+    here every energy of the grid goes through one Lopez-Sancho launch per lead
+    and one RGF launch that reduces diag(G_qq) and diag(G_qN Gamma_R G_qN^H)
+    inside the sweep (``DeviceProperty.orbital_spectra``); the per-atom sums
+    and the electron/hole selection are tensor ops on the GPU.
+
+    The weights and nodes follow the reference's dtypes: ``dE * torch.ones``
+    and ``gauss_xw`` of ``torch.scalar_tensor`` limits are float32, as there.
+    Two reference branches cannot run as written, and run here as intended:
+    with ``block_tridiagonal=True`` the reference reads ``gr_lc``, which its
+    ``cal_green_function`` call never requests (density.py:293-294, 304), and
+    without Dirichlet leads it passes ``save=False``, which
+    ``LeadProperty.self_energy`` does not accept (density.py:278-279); here the
+    last block column enters through the sweep's reduction and the lead
+    self-energies are recomputed, never loaded, without Dirichlet leads.
+    """
+
+    def __init__(self, n_gauss=None, integrate_way: str = "direct", e_grid=None):
+        super().__init__()
+        self.n_gauss = n_gauss
+        self.e_grid = e_grid
+        self.integrate_way = integrate_way
+        self.xs = None
+        self.wlg = None
+        self.e_grid_Fiori = None
+        if integrate_way == "gauss":
+            assert self.n_gauss is not None, "n_gauss must be set in the Fiori class with gauss integration"
+            self.xs, self.wlg = gauss_xw(xl=torch.scalar_tensor(e_grid[0]), xu=torch.scalar_tensor(e_grid[-1]),
+                                         n=self.n_gauss)
+            self.e_grid_Fiori = e_grid
+            integrate_range, pre_factor = self.xs, self.wlg
+        elif integrate_way == "direct":
+            dE = e_grid[1] - e_grid[0]
+            integrate_range = e_grid
+            pre_factor = dE * torch.ones(len(e_grid))
+        else:
+            raise ValueError("integrate_way only supports 'gauss' and 'direct' in this version")
+        self.integrate_range = integrate_range
+        self.pre_factor = pre_factor
+
+    def density_integrate_Fiori(self, e_grid, kpoint, Vbias, block_tridiagonal, subblocks, integrate_way, deviceprop,
+                                device_atom_norbs, potential_at_atom, with_Dirichlet_leads, free_charge, E_ref,
+                                eta_lead=1e-5, eta_device=1e-5, self_energy_save_path=None):
+        """Add this k-point's free charge per atom into ``free_charge[str(kpoint)]`` (in place).
+
+        ``e_grid`` and ``integrate_way`` are accepted for the reference's signature; the grid
+        and weights are the ones built in ``__init__``, as in the reference.  ``subblocks`` is
+        implied by the device blocks: orbitals are numbered through the blocks in order."""
+        E = torch.as_tensor(self.integrate_range)
+        B = E.shape[0]
+        e_arg = E if B > 1 else E[0]  # one energy: the scalar contract ([n, n] self-energies)
+        for lead in (deviceprop.lead_L, deviceprop.lead_R):
+            if with_Dirichlet_leads:
+                lead.self_energy(kpoint=kpoint, energy=e_arg, eta_lead=eta_lead, save_path=self_energy_save_path)
+            else:
+                lead.se = lead.self_energy_cal(kpoint, e_arg, eta_lead=eta_lead)
+        g, a_R = deviceprop.orbital_spectra(energy=e_arg, kpoint=kpoint, eta_device=eta_device,
+                                            block_tridiagonal=block_tridiagonal, Vbias=Vbias)
+        dev = g.device
+        a_L = -2.0 * g.imag - a_R  # diag of i(G - G^H) - A_R
+        e = E.to(dev)
+        fL = torch.as_tensor(deviceprop.lead_L.fermi_dirac(e + E_ref)).to(dev).reshape(B, 1)
+        fR = torch.as_tensor(deviceprop.lead_R.fermi_dirac(e + E_ref)).to(dev).reshape(B, 1)
+        gn = a_L * fL + a_R * fR
+        gp = a_L + a_R - gn
+        norbs = [int(x) for x in device_atom_norbs]
+        atom_of_orb = torch.as_tensor(np.repeat(np.arange(len(norbs)), norbs), device=dev)
+        gn_atom = torch.zeros(B, len(norbs), dtype=gn.dtype, device=dev).index_add_(1, atom_of_orb, gn)
+        gp_atom = torch.zeros(B, len(norbs), dtype=gp.dtype, device=dev).index_add_(1, atom_of_orb, gp)
+        Ei = torch.as_tensor(-1 * potential_at_atom).to(dev).reshape(1, -1)
+        pre = torch.as_tensor(self.pre_factor).to(dev)
+        c_e = (pre * 2 * (-1) / 2 / torch.pi).reshape(B, 1)
+        c_h = (pre * 2 * 1 / 2 / torch.pi).reshape(B, 1)
+        charge = torch.where(e.reshape(B, 1) >= Ei, c_e * gn_atom, c_h * gp_atom).sum(0)
+        fc = free_charge[str(kpoint)]
+        fc += charge.to(device=fc.device, dtype=fc.dtype)
+
+    def get_subblock_index(self, subblocks, atom_index, device_atom_norbs):
+        """Blocks holding atom ``atom_index``'s orbitals, with the first orbital's offset in the
+        first of them and the end offset in the last (density.py:362-395)."""
+        edges = np.concatenate([[0], np.cumsum(subblocks)])
+        first = int(sum(device_atom_norbs[:atom_index]))
+        last = first + int(device_atom_norbs[atom_index])
+        i = int(np.searchsorted(edges, first, side="right")) - 1
+        blocks = [i]
+        while last > edges[blocks[-1] + 1]:
+            blocks.append(blocks[-1] + 1)
+        return blocks, first - int(edges[i]), last - int(edges[blocks[-1]])

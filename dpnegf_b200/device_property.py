@@ -79,14 +79,9 @@ class DeviceProperty(object):
         self._geom = rgf_plan.Geometry([rgf_plan.DeviceBlocks(self.hd, self.hu, self.hl, self.sd, self.su,
                                                               self.sl)], device=dev)
 
-    def cal_green_function(self, energy, kpoint, eta_device=0., block_tridiagonal=True, Vbias=None,
-                           HS_inmem: bool = True, need_lesser: bool = False, need_greater: bool = False,
-                           need_gr_lc: bool = False):
-        """Green's functions (and fused T, DOS, LDOS) at ``energy`` (scalar or [B]) for ``kpoint``."""
-        # the reference passes s_out=None to recursive_gf here (device_property.py:283), whose greater
-        # branch then fails its list check (recursive_green_cal.py:67 / :268): same error
-        assert not need_greater, \
-            "Greater Green's function calculation requires s_out to be a list of coupling matrices"
+    def _prepare(self, energy, kpoint, block_tridiagonal, Vbias):
+        """Energy batch, potential and H/S refresh, self-energy checks of ``cal_green_function``
+        (reference device_property.py:170-255)."""
         assert len(np.array(kpoint).reshape(-1)) == 3
         dev = self._compute_device()
         energy = torch.as_tensor(energy, dtype=torch.complex128, device=dev)
@@ -144,6 +139,30 @@ class DeviceProperty(object):
                 raise ValueError("Right Lead Self Energy size is larger than the last Hamiltonian Block.")
         seLb = seL if seL.ndim == 3 else seL.unsqueeze(0)
         seRb = seR if seR.ndim == 3 else seR.unsqueeze(0)
+        return energy, B, batched_mode, seLb, seRb, (idx0, idy0, idx1, idy1)
+
+    def orbital_spectra(self, energy, kpoint, eta_device=0., block_tridiagonal=True, Vbias=None):
+        """Per-orbital diag(G_qq) and diag(G_qN Gamma_R G_qN^H) over every block at ``energy``
+        (scalar or [B]), reduced inside one sweep without materialising Green's-function blocks:
+        ``([B, n_orb] complex, [B, n_orb] float64)``.  The self-energies are the leads' current
+        ``se`` as in ``cal_green_function``; Gamma_R = i(Sigma_R - Sigma_R^H) in the last block's
+        bottom-right corner."""
+        energy, B, _, seLb, seRb, _ = self._prepare(energy, kpoint, block_tridiagonal, Vbias)
+        res = rgf_plan.run(self._geom, [energy], [seLb], [seRb], eta=eta_device, E_ref=self.E_ref,
+                           outputs=(), orb_g=True, orb_ar=True)
+        n_orb = int(self._geom.n_orb[0])
+        return res.orb_g.view(B, n_orb), res.orb_ar.view(B, n_orb)
+
+    def cal_green_function(self, energy, kpoint, eta_device=0., block_tridiagonal=True, Vbias=None,
+                           HS_inmem: bool = True, need_lesser: bool = False, need_greater: bool = False,
+                           need_gr_lc: bool = False):
+        """Green's functions (and fused T, DOS, LDOS) at ``energy`` (scalar or [B]) for ``kpoint``."""
+        # the reference passes s_out=None to recursive_gf here (device_property.py:283), whose greater
+        # branch then fails its list check (recursive_green_cal.py:67 / :268): same error
+        assert not need_greater, \
+            "Greater Green's function calculation requires s_out to be a list of coupling matrices"
+        energy, B, batched_mode, seLb, seRb, corners = self._prepare(energy, kpoint, block_tridiagonal, Vbias)
+        idx0, idy0, idx1, idy1 = corners
 
         s_in = None
         if need_lesser:

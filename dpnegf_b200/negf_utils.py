@@ -13,9 +13,13 @@ import torch
 
 
 def gauss_xw(xl, xu, n=100):
-    """Gauss-Legendre points and weights on [xl, xu] (same layout as the reference)."""
-    xu = torch.as_tensor(xu, dtype=torch.float64)
-    xl = torch.as_tensor(xl, dtype=torch.float64, device=xu.device)
+    """Gauss-Legendre points and weights on [xl, xu] (same layout as the reference), in the
+    floating dtype of ``xu`` as the reference computes them (a float32 ``xu``, e.g. from
+    ``torch.scalar_tensor`` of a Python float, gives float32 nodes and weights)."""
+    xu = torch.as_tensor(xu)
+    if not xu.is_floating_point():
+        xu = xu.to(torch.float64)
+    xl = torch.as_tensor(xl, dtype=xu.dtype, device=xu.device)
     nd = xu.ndim
     x, w = np.polynomial.legendre.leggauss(n)
     x = torch.tensor(x, dtype=xu.dtype, device=xu.device)[(...,) + (None,) * nd]

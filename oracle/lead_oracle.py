@@ -140,3 +140,73 @@ def current_nscf(energy_grid, tc, efermi, kBT):
     cc = [simpson(y=(f(energy_grid + efermi, efermi - vm + dv) - f(energy_grid + efermi, efermi - vm - dv)) * tc,
                   x=energy_grid) for dv in vv * 0.5]
     return vv, np.array(cc)
+
+
+def fiori_subblock_index(subblocks, atom_index, norbs):
+    """Blocks holding an atom's orbitals, with the start offset in the first of them and the end
+    offset in the last (negf/density.py:362-395): scan the block edges for the block holding the
+    first orbital, then extend block by block until the last orbital is covered."""
+    edges = [0]
+    for n in subblocks:
+        edges.append(edges[-1] + int(n))
+    first = int(sum(norbs[:atom_index]))
+    last = first + int(norbs[atom_index])
+    for i in range(len(edges) - 1):
+        if edges[i] <= first and last <= edges[i + 1]:
+            return [i], first - edges[i], last - edges[i]
+        if edges[i] <= first < edges[i + 1] < last:
+            blocks = [i]
+            for j in range(i + 1, len(edges) - 1):
+                blocks.append(j)
+                if last <= edges[j + 1]:
+                    return blocks, first - edges[i], last - edges[j]
+    raise ValueError(f"atom {atom_index} lies outside the blocks")
+
+
+def fiori_free_charge(energies, pre_factor, blocks, left_se, right_se, eta_device, E_ref_device, fermi_L, fermi_R,
+                      E_ref, norbs, potential_at_atom, block_tridiagonal, subblocks):
+    """Restatement of ``Fiori.density_integrate_Fiori`` (negf/density.py:268-360), one energy at a time.
+
+    ``blocks`` = (hd, hu, hl, sd, su, sl); ``left_se`` / ``right_se`` hold one self-energy per
+    energy.  For each energy: A_R = G Gamma_R G^H from the full block (dense device) or from the
+    last block column G_qN (BTD device), A_L = i(G_qq - G_qq^H) - A_R, G^n = A_L f_L + A_R f_R,
+    G^p = A_L + A_R - G^n, f at E + E_ref; then per atom  w (-1/pi) Tr G^n  if E >= -potential
+    (electrons) else  w (1/pi) Tr G^p  (holes), the trace taken over the atom's orbitals block by
+    block as the reference slices them.  Returns the complex [n_atoms] charge."""
+    from . import rgf_oracle
+    hd, hu, hl, sd, su, sl = blocks
+    charge = np.zeros(len(norbs), dtype=np.complex128)
+    edges = np.concatenate([[0], np.cumsum(norbs)])
+    for i, e in enumerate(energies):
+        out = rgf_oracle.rgf(complex(e), hl, hd, hu, sd, su, sl, left_se[i], right_se[i], E_ref=E_ref_device,
+                             eta=eta_device, need_gr_lc=True)
+        grd = [x[0] for x in out["grd"]]
+        gam = rgf_oracle.gamma_from_se(np.asarray(right_se[i]))
+        ty = grd[-1].shape[-1]
+        x1 = min(gam.shape[0], ty)
+        if not block_tridiagonal:
+            GR = np.zeros((ty, ty), dtype=np.complex128)
+            GR[ty - x1:, ty - x1:] = gam[gam.shape[0] - x1:, gam.shape[1] - x1:]
+            A_R = [grd[0] @ GR @ grd[0].conj().T]
+        else:
+            gR = gam[gam.shape[0] - x1:, gam.shape[1] - x1:]
+            A_R = [c[0] @ gR @ c[0].conj().T for c in out["gr_lc"]]
+        A_L = [1j * (g - g.conj().T) - a for g, a in zip(grd, A_R)]
+        fl, fr = fermi_L(e + E_ref), fermi_R(e + E_ref)
+        gn = [al * fl + ar * fr for al, ar in zip(A_L, A_R)]
+        gp = [al + ar - n for al, ar, n in zip(A_L, A_R, gn)]
+        for a, Ei in enumerate(-1 * np.asarray(potential_at_atom)):
+            electron = e >= Ei
+            M = gn if electron else gp
+            coef = pre_factor[i] * 2 * (-1) / 2 / np.pi if electron else pre_factor[i] * 2 * 1 / 2 / np.pi
+            if not block_tridiagonal:
+                tr = np.trace(M[0][edges[a]:edges[a + 1], edges[a]:edges[a + 1]])
+            else:
+                bl, s0, s1 = fiori_subblock_index(subblocks, a, norbs)
+                if len(bl) == 1:
+                    tr = np.trace(M[bl[0]][s0:s1, s0:s1])
+                else:
+                    tr = np.trace(M[bl[0]][s0:, s0:]) + np.trace(M[bl[-1]][:s1, :s1])
+                    tr = tr + sum(np.trace(M[b]) for b in bl[1:-1])
+            charge[a] += coef * tr
+    return charge

@@ -23,7 +23,15 @@ seeded inputs together with the reference's own outputs:
   adjoint_dos_*.npz  the same for sum_E (wT_E T(E) + wD_E DOS(E)), the DOS formed
                   from the reference's blocks as ``_cal_dos_`` does
                   (device_property.py:408-439): the summed onsite density over
-                  an energy window when wD carries occupation x quadrature weights.
+                  an energy window when wD carries occupation x quadrature weights;
+  fiori_*.npz     ``Fiori.density_integrate_Fiori`` (negf/density.py:268-360):
+                  per-atom free charge on a direct and a Gauss grid, dense
+                  device (``block_tridiagonal=False``) and BTD device.  The
+                  reference's BTD branch reads ``gr_lc`` without requesting it,
+                  so for that case the fake device property asks
+                  ``cal_green_function`` for it (``need_gr_lc=True``); the
+                  leads serve seeded self-energies per grid energy.  Also the
+                  reference's ``get_subblock_index`` for every atom.
 The fixtures are small (tens of KB) and are committed; the GPU box never needs
 the reference sources.
 """
@@ -173,6 +181,78 @@ def _devprop_case(dp_mod, name, dims, B, seed, norbs, need_lesser=True):
     np.savez_compressed(os.path.join(HERE, f"devprop_{name}.npz"), **d)
 
 
+class _TableLead(_FakeLead):
+    """Lead whose ``self_energy`` serves a seeded table, one matrix per grid energy."""
+
+    def __init__(self, mu, energies, table):
+        super().__init__(mu)
+        self._keys = [float(x) for x in energies]
+        self._table = table
+
+    def self_energy(self, kpoint, energy, eta_lead=1e-5, save_path=None, **kw):
+        self.se = self._table[self._keys.index(float(energy))]
+
+
+def _fiori_case(dp_mod, dens_mod, name, dims, norbs, block_tridiagonal, integrate_way, seed, nL, nR):
+    dev = workload.random_device(0, 0, seed=seed, block_dims=dims)
+    e_grid = torch.linspace(-0.4, 0.4, 9, dtype=torch.float64)
+    fi = dens_mod.Fiori(n_gauss=6 if integrate_way == "gauss" else None, integrate_way=integrate_way, e_grid=e_grid)
+    E = fi.integrate_range
+    B = len(E)
+    seL = workload.random_self_energy(B, nL, seed=seed + 1)
+    seR = workload.random_self_energy(B, nR, seed=seed + 2)
+    dp = dp_mod.DeviceProperty.__new__(dp_mod.DeviceProperty)
+    dp.greenfuncs = 0
+    dp.hamiltonian = _FakeHamiltonian(dev)
+    dp.structure = None
+    dp.results_path = "/nonexistent-negf-results"
+    dp.cdtype = torch.complex128
+    dp.rgf_device = "cpu"
+    dp.kBT = 0.025
+    dp.e_T = 300.0
+    dp.chemiPot = None
+    dp.E_ref = 0.05
+    dp.kpoint = None
+    dp.newK_flag = None
+    dp.newV_flag = None
+    dp.lead_L = _TableLead(0.1, E, seL)
+    dp.lead_R = _TableLead(-0.1, E, seR)
+    if block_tridiagonal:
+        plain = dp.cal_green_function
+        dp.cal_green_function = lambda **kw: plain(need_gr_lc=True, **kw)
+    gen = torch.Generator().manual_seed(seed + 3)
+    pot = torch.rand(len(norbs), generator=gen, dtype=torch.float64) * 0.6 - 0.3
+    k = [0.0, 0.0, 0.0]
+    fc = {str(k): torch.zeros(len(norbs), dtype=torch.complex128)}
+    fi.density_integrate_Fiori(e_grid=e_grid, kpoint=k, Vbias=None, block_tridiagonal=block_tridiagonal,
+                               subblocks=dims, integrate_way=integrate_way, deviceprop=dp,
+                               device_atom_norbs=norbs, potential_at_atom=pot, with_Dirichlet_leads=True,
+                               free_charge=fc, E_ref=0.05, eta_lead=1e-5, eta_device=1e-6)
+    d = {}
+    _put(d, "dims", np.array(dims))
+    _put(d, "norbs", np.array(norbs))
+    _put(d, "block_tridiagonal", np.array(block_tridiagonal))
+    _put(d, "integrate_way", np.array(integrate_way))
+    _put(d, "e_grid", e_grid)
+    _put(d, "integrate_range", E)
+    _put(d, "pre_factor", fi.pre_factor)
+    for key in ("hd", "hu", "hl", "sd", "su", "sl"):
+        _put(d, key, getattr(dev, key))
+    _put(d, "left_se", seL)
+    _put(d, "right_se", seR)
+    _put(d, "potential_at_atom", pot)
+    _put(d, "E_ref", np.array(0.05))
+    _put(d, "eta_device", np.array(1e-6))
+    _put(d, "muL", np.array(0.1))
+    _put(d, "muR", np.array(-0.1))
+    _put(d, "kBT", np.array(0.025))
+    _put(d, "out/free_charge", fc[str(k)])
+    for a in range(len(norbs)):
+        blk, s0, s1 = fi.get_subblock_index(dims, a, norbs)
+        _put(d, f"out/subblock/{a}", np.array(list(blk) + [s0, s1]))
+    np.savez_compressed(os.path.join(HERE, f"fiori_{name}.npz"), **d)
+
+
 def _lopez_cases(sg_mod):
     d = {}
     chain = workload.chain_device(L=4)
@@ -305,7 +385,7 @@ def _adjoint_dos_case(rgf_mod, name, dims, B, seed, with_t, eta=1e-5):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default=ref_import.DEFAULT_REF_ROOT)
-    ap.add_argument("--only", default=None, help="regenerate one family: rgf, devprop, lopez, ozaki, adjoint")
+    ap.add_argument("--only", default=None, help="regenerate one family: rgf, devprop, lopez, ozaki, adjoint, fiori")
     args = ap.parse_args()
     torch.set_num_threads(1)  # the container's threaded batched zgesv can hang
     rgf_mod = ref_import.load("recursive_green_cal", args.ref_root)
@@ -313,6 +393,7 @@ def main():
     dp_mod = ref_import.load("device_property", args.ref_root)
     oz_mod = ref_import.load("ozaki_res_cal", args.ref_root)
     nu_mod = ref_import.load("negf_utils", args.ref_root)
+    dens_mod = ref_import.load("density", args.ref_root)
 
     want = lambda fam: args.only in (None, fam)
     if want("rgf"):
@@ -338,6 +419,11 @@ def main():
         _adjoint_dos_case(rgf_mod, "nonuniform", [6, 9, 5, 7], 3, seed=24, with_t=False)
         _adjoint_dos_case(rgf_mod, "uniform_with_t", [10] * 5, 2, seed=25, with_t=True)
         _adjoint_dos_case(rgf_mod, "single_block", [8], 2, seed=26, with_t=False)
+    if want("fiori"):
+        _fiori_case(dp_mod, dens_mod, "dense_direct", [9], [2, 3, 4], False, "direct", seed=31, nL=3, nR=4)
+        _fiori_case(dp_mod, dens_mod, "dense_gauss", [9], [2, 3, 4], False, "gauss", seed=32, nL=3, nR=4)
+        _fiori_case(dp_mod, dens_mod, "btd_direct", [4, 5, 4], [2, 3, 1, 3, 4], True, "direct", seed=33,
+                    nL=3, nR=4)
     print("golden fixtures written to", HERE)
 
 

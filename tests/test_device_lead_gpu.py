@@ -327,3 +327,64 @@ def test_bloch_lead_self_energy_matches_reference_loop():
         Es = e + 0.1
         ref = (Es * SDL.numpy() - HDL.numpy()) @ sgf[:2 * n, :2 * n] @ (Es * SDL.numpy().conj().T - HDL.numpy().conj().T)
         assert _rel(lp.se[i], ref) < 1e-9
+
+
+class TableLead(FakeLead):
+    """Lead serving a fixture's self-energies, one per grid energy, scalar or batched."""
+
+    def __init__(self, mu, energies, table):
+        super().__init__(mu)
+        self._keys = [float(x) for x in np.asarray(energies)]
+        self._table = torch.as_tensor(table)
+
+    def _lookup(self, energy):
+        e = torch.as_tensor(energy).reshape(-1).tolist()
+        idx = [min(range(len(self._keys)), key=lambda i: abs(self._keys[i] - x)) for x in e]
+        se = self._table[idx]
+        return se if torch.as_tensor(energy).ndim else se[0]
+
+    def self_energy(self, kpoint, energy, eta_lead=1e-5, save_path=None, **kw):
+        self.se = self._lookup(energy)
+
+    def self_energy_cal(self, kpoint, energy, eta_lead=1e-5, **kw):
+        return self._lookup(energy)
+
+
+@pytest.mark.parametrize("case", ["fiori_dense_direct", "fiori_dense_gauss", "fiori_btd_direct"])
+@pytest.mark.parametrize("dirichlet", [True, False])
+def test_fiori_free_charge_matches_reference_fixture(case, dirichlet):
+    """Fiori per-atom free charge (one lead launch per lead, one sweep over the grid) against the
+    reference's own run: 1e-10 relative on the float64 grid, 1e-6 on the float32 Gauss grid
+    (float32 Fermi factors on the GPU may differ from the host's by an ulp)."""
+    from dpnegf_b200 import workload
+    from dpnegf_b200.density import Fiori
+    from dpnegf_b200.device_property import DeviceProperty
+    g = Golden(case)
+    dims, norbs = [int(n) for n in g["dims"]], [int(n) for n in g["norbs"]]
+    bt = bool(g["block_tridiagonal"])
+    way = str(g["integrate_way"])
+    e_grid = torch.as_tensor(g["e_grid"])
+    fi = Fiori(n_gauss=6 if way == "gauss" else None, integrate_way=way, e_grid=e_grid)
+    assert fi.pre_factor.dtype == torch.float32
+    np.testing.assert_array_equal(fi.pre_factor.numpy(), g["pre_factor"])
+    np.testing.assert_array_equal(torch.as_tensor(fi.integrate_range).numpy(), g["integrate_range"])
+    dev = workload.BTDDevice(*[[torch.as_tensor(x) for x in g[k]] for k in ("hd", "hu", "hl", "sd", "su", "sl")])
+    dp = DeviceProperty(FakeHamiltonian(dev, norbs), None, "", e_T=300, E_ref=float(g["E_ref"]))
+    dp.kBT = float(g["kBT"])
+    dp.set_leadLR(TableLead(float(g["muL"]), g["integrate_range"], g["left_se"]),
+                  TableLead(float(g["muR"]), g["integrate_range"], g["right_se"]))
+    k = [0.0, 0.0, 0.0]
+    fc = {str(k): torch.zeros(len(norbs), dtype=torch.complex128, device="cuda")}
+    fi.density_integrate_Fiori(e_grid=e_grid, kpoint=k, Vbias=None, block_tridiagonal=bt, subblocks=dims,
+                               integrate_way=way, deviceprop=dp, device_atom_norbs=norbs,
+                               potential_at_atom=torch.as_tensor(g["potential_at_atom"]),
+                               with_Dirichlet_leads=dirichlet, free_charge=fc, E_ref=float(g["E_ref"]),
+                               eta_lead=1e-5, eta_device=float(g["eta_device"]))
+    tol = 1e-6 if way == "gauss" else 1e-10
+    want = g["out/free_charge"].real
+    got = fc[str(k)].real.cpu().numpy()
+    print(f"{case}: Fiori free charge relative error {np.abs(got - want).max() / np.abs(want).max():.2e}")
+    assert np.abs(got - want).max() < tol * np.abs(want).max()
+    for a in range(len(norbs)):
+        bl, s0, s1 = fi.get_subblock_index(dims, a, norbs)
+        assert list(bl) + [s0, s1] == [int(x) for x in g[f"out/subblock/{a}"]]

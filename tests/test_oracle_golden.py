@@ -110,3 +110,36 @@ def test_ozaki_and_gauss_match_reference():
     x, w = lead_oracle.gauss_xw(-0.4, 0.5, 10)
     _close(x, g["gauss/x"], atol=1e-15, rtol=0)
     _close(w, g["gauss/w"], atol=1e-15, rtol=0)
+
+
+FIORI_CASES = ("fiori_dense_direct", "fiori_dense_gauss", "fiori_btd_direct")
+
+
+def _fiori_oracle(g):
+    mu_l, mu_r, kBT = float(g["muL"]), float(g["muR"]), float(g["kBT"])
+    blocks = tuple(g[k] for k in ("hd", "hu", "hl", "sd", "su", "sl"))
+    return lead_oracle.fiori_free_charge(
+        g["integrate_range"], g["pre_factor"], blocks, g["left_se"], g["right_se"], float(g["eta_device"]),
+        float(g["E_ref"]), lambda x: 1.0 / (1.0 + np.exp((x - mu_l) / kBT)),
+        lambda x: 1.0 / (1.0 + np.exp((x - mu_r) / kBT)), float(g["E_ref"]), [int(n) for n in g["norbs"]],
+        g["potential_at_atom"], bool(g["block_tridiagonal"]), [int(n) for n in g["dims"]])
+
+
+@pytest.mark.parametrize("case", FIORI_CASES)
+def test_fiori_free_charge_matches_reference(case):
+    """The Fiori charge restatement against the reference's own Fiori run, within 1e-10 relative.
+    The Gauss grid is float32 in the reference (nodes and weights from float32 limits, Fermi
+    factors in float32); numpy 2 keeps the same float32 arithmetic here."""
+    g = Golden(case)
+    got = _fiori_oracle(g)
+    want = g["out/free_charge"]
+    assert np.abs(got.real - want.real).max() < 1e-10 * np.abs(want.real).max()
+
+
+@pytest.mark.parametrize("case", FIORI_CASES)
+def test_fiori_subblock_index_matches_reference(case):
+    g = Golden(case)
+    dims, norbs = [int(n) for n in g["dims"]], [int(n) for n in g["norbs"]]
+    for a in range(len(norbs)):
+        bl, s0, s1 = lead_oracle.fiori_subblock_index(dims, a, norbs)
+        assert list(bl) + [s0, s1] == [int(x) for x in g[f"out/subblock/{a}"]]

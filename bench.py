@@ -52,8 +52,10 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision and adjoint legs")
     ap.add_argument("--refine-steps", type=int, default=3)
     ap.add_argument("--configs", default="",
-                    help="extra legs, comma separated: 'uneven' (the 512-device uneven batch, 128 devices) "
-                         "and 'scf' (b=512 SCF loop captured as a CUDA graph); not in the default run")
+                    help="extra legs, comma separated: 'uneven' (the 512-device uneven batch, 128 devices), "
+                         "'leads' (its lead decimation alone, --lead-devices devices) and 'scf' (b=512 SCF "
+                         "loop captured as a CUDA graph); not in the default run")
+    ap.add_argument("--lead-devices", type=int, default=128, help="devices whose leads the 'leads' leg decimates")
     ap.add_argument("--inverse", default=None, choices=["gj", "block"],
                     help="Schur-complement inverse: pivoted Gauss-Jordan or recursive 2x2 blocks "
                          "(default: the autotuned scheme, else block)")
@@ -317,18 +319,21 @@ ETA_LEAD_SYNTH = 1e-3
 ETA_LEAD_NOTE = "lead eta 1e-3 (the random dense leads miss the decimation residual criterion at 1e-5)"
 
 
-def uneven_leg(torch, n_devices=128, seed=2024):
-    """The uneven batch: devices with b ~ U{16..256} (step 16) and L ~ U{8..64}, energies = the far
-    pole + 64 Ozaki poles at kT = 25 meV + 256 Gauss-Legendre points of the 0.3 V bias window;
-    every lead at every energy in one decimation launch, every (device, energy) item in one
-    persistent sweep (Ozaki.uneven_batch).  FP64, mixed, and mixed + FP64-residual refinement,
-    the mixed runs checked against FP64; the decimation phase also timed alone.  ``n_devices`` of the 512 (the full batch's self-energies alone need
-    about 100 GB; it runs as chunks of this size)."""
+def _ls_flops(n, iters):
+    """Algorithmic FP64 work of one decimation: 8 (7/3 + 4) n^3 per doubling step (one solve with
+    2n right-hand sides, four products) times the steps taken, plus 16 n^3 for g_s and Sigma."""
+    return 8.0 * (7.0 / 3.0 + 4.0) * n ** 3 * iters + 16.0 * n ** 3
+
+
+def _uneven_inputs(torch, n_devices, seed):
+    """Devices with b ~ U{16..256} (step 16) and L ~ U{8..64}, their edge-block leads, and the
+    energies: the far pole + 64 Ozaki poles at kT = 25 meV + 256 Gauss-Legendre points of the
+    0.3 V bias window."""
     import numpy as np
     from dpnegf_b200 import rgf_plan, workload
     from dpnegf_b200.density import Ozaki
     from dpnegf_b200.scf import ozaki_weights
-    from dpnegf_b200.surface_green import LeadArena, LeadBlocks, self_energies
+    from dpnegf_b200.surface_green import LeadBlocks
     rng = np.random.default_rng(seed)
     devs, leads, work = [], [], 0.0
     for d in range(n_devices):
@@ -343,11 +348,47 @@ def uneven_leg(torch, n_devices=128, seed=2024):
     oz = Ozaki(R=1e6, M_cut=64, n_gauss=256)
     fL = lambda x: 1.0 / (1.0 + torch.exp((x - (mu_L - vL)) / kBT))
     fR = lambda x: 1.0 / (1.0 + torch.exp((x - (mu_L - vR)) / kBT))
-    nE = 1 + len(oz.poles) + 256
-    timed = lambda fn: _timed(torch, fn)
-    # the decimation phase alone: every lead at every energy, one launch
     z = ozaki_weights(oz.poles.numpy(), oz.residues.numpy(), oz.R, 256, kBT, mu_L, vL=vL, vR=vR, fermi_L=fL,
                       fermi_R=fR)[0]
+    return dict(devs=devs, leads=leads, work=work, kBT=kBT, mu_L=mu_L, vL=vL, vR=vR, oz=oz, fL=fL, fR=fR, z=z)
+
+
+def leads_leg(torch, peak, n_devices=128, seed=2024):
+    """The uneven batch's decimation phase alone: both leads of every device at every energy in one
+    Lopez-Sancho launch, timed with CUDA events, with its algorithmic FP64 rate against the
+    measured DGEMM peak (per-item doubling steps from the kernel's own iteration counts)."""
+    import numpy as np
+    from dpnegf_b200.surface_green import LeadArena, self_energies
+    u = _uneven_inputs(torch, n_devices, seed)
+    nE = len(u["z"])
+    arena = LeadArena([ld for pair in u["leads"] for ld in pair])
+    idx = np.repeat(np.arange(2 * n_devices), nE)
+    self_energies(arena, idx[:2 * nE], np.tile(u["z"], 2), ETA_LEAD_SYNTH)  # warm-up: module load, first launch
+    res, ms = _timed(torch, lambda: self_energies(arena, idx, np.tile(u["z"], 2 * n_devices), ETA_LEAD_SYNTH))
+    n = np.array([arena.shapes[i][0] for i in idx], dtype=np.float64)
+    flops = float(_ls_flops(n, res.iters.astype(np.float64)).sum())
+    ach = flops / (ms * 1e-3) / 1e12
+    return {"items": int(len(idx)), "n": "16..256", "seconds": ms * 1e-3, "value": len(idx) / (ms * 1e-3),
+            "unit": "decimations/s", "mean_iters": float(res.iters.mean()), "max_iters": int(res.iters.max()),
+            "roofline": {"achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+                         "algorithmic": "8 (7/3 + 4) n^3 per doubling step x steps + 16 n^3 per item"},
+            "note": ETA_LEAD_NOTE}
+
+
+def uneven_leg(torch, n_devices=128, seed=2024):
+    """The uneven batch (``_uneven_inputs``): every lead at every energy in one decimation launch,
+    every (device, energy) item in one persistent sweep (Ozaki.uneven_batch).  FP64, mixed, and
+    mixed + FP64-residual refinement, the mixed runs checked against FP64; the decimation phase
+    also timed alone.  ``n_devices`` of the 512 (the full batch's self-energies alone need about
+    100 GB; it runs as chunks of this size)."""
+    import numpy as np
+    from dpnegf_b200.surface_green import LeadArena, self_energies
+    u = _uneven_inputs(torch, n_devices, seed)
+    devs, leads, work, oz = u["devs"], u["leads"], u["work"], u["oz"]
+    kBT, mu_L, vL, vR, fL, fR, z = u["kBT"], u["mu_L"], u["vL"], u["vR"], u["fL"], u["fR"], u["z"]
+    nE = len(z)
+    timed = lambda fn: _timed(torch, fn)
+    # the decimation phase alone: every lead at every energy, one launch
     arena = LeadArena([ld for pair in leads for ld in pair])
     ms_lead = timed(lambda: self_energies(arena, np.repeat(np.arange(2 * n_devices), nE),
                                           np.tile(z, 2 * n_devices), ETA_LEAD_SYNTH))[1]
@@ -422,7 +463,10 @@ def scf_leg(torch, peak):
     ach = 72.0 * b ** 3 * L * pts / (ms["fp64"] * 1e-3) / 1e12
     rel = lambda x, y: float((x - y).abs().max() / max(float(y.abs().max()), 1e-300))
     return {"b": b, "L": L, "energies": nE, "iterations": iters,
-            "lead_decimation": {"items": 2 * nE, "seconds": t_lead * 1e-3, "n": b},
+            "lead_decimation": {"items": 2 * nE, "seconds": t_lead * 1e-3, "n": b,
+                                "mean_iters": float(ls.iters.mean()),
+                                "tflops_algorithmic": float(_ls_flops(float(b), ls.iters.astype(np.float64)).sum())
+                                / (t_lead * 1e-3) / 1e12},
             "fp64": {"value": pts / (ms["fp64"] * 1e-3), "unit": UNIT, "seconds": ms["fp64"] * 1e-3,
                      "roofline": {"achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak}},
             "mixed": {"value": pts / (ms["mixed"] * 1e-3), "unit": UNIT, "seconds": ms["mixed"] * 1e-3,
@@ -689,6 +733,8 @@ def main():
     extra = {}
     if rank == 0 and args.configs:
         wanted = [x.strip() for x in args.configs.split(",") if x.strip()]
+        if "leads" in wanted:
+            extra["config3_leads"] = leads_leg(torch, peak, n_devices=args.lead_devices)
         if "uneven" in wanted:
             extra["config3_uneven"] = uneven_leg(torch)
         if "scf" in wanted:

@@ -79,7 +79,9 @@ NEGF_DEV void gemm_ls(cplx* smem, int M, int N, int K, const cplx* A, int64_t ld
   GemmArgs g = gemm_args(M, N, K, A, lda, B, ldb, C, ldc);
   g.alpha = alpha;
   if (D) { g.D = D; g.ldd = ldd; g.beta = beta; g.use_d = true; }
-  cta_gemm<OPA, OPB, false>(g, smem);  // conventional 4M products: see warp_mma_3m
+  // conventional 4M products (see warp_mma_3m); lead blocks come in every size, so warps
+  // outside the product skip their MMAs
+  cta_gemm<OPA, OPB, false, true>(g, smem);
 }
 
 NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, char* smem_raw, double* red) {

@@ -416,54 +416,49 @@ def uneven_leg(torch, n_devices=128, seed=2024):
                     "72 b^3 L per item over the FP64 call's time less the decimation's; " + ETA_LEAD_NOTE})
 
 
-def scf_leg(torch, peak):
-    """b=512, L=40: lead decimation on 512 x 512 blocks, then 10 timed SCF iterations of damped (0.3)
-    onsite shifts V = 0.5 (n - n0) around the sweep, the iteration replayed as a CUDA graph
-    (scf.ScfLoop); energies = far pole + 64 Ozaki poles + 231 bias-window points (296 = two
-    waves of the persistent CTAs).  FP64 and mixed; the mixed density checked against FP64."""
+def scf_leg(torch, peak, nk=8):
+    """b=512, L=40 at ``nk`` k-points (distinct H(k), S(k) realisations, equal weights): lead
+    decimation on 512 x 512 blocks, then 10 timed SCF iterations of damped (0.3) onsite shifts
+    V = 0.5 (n - n0) around one sweep over every (k, energy) item, the iteration replayed as a CUDA
+    graph (scf.ScfLoop); energies per k = far pole + 16 Ozaki poles + 20 bias-window points, so
+    8 k x 37 = 296 items per iteration (two waves of the persistent CTAs).  FP64 and mixed; the
+    mixed density checked against FP64."""
     import numpy as np
     from dpnegf_b200 import rgf_plan, workload
     from dpnegf_b200.ozaki_res_cal import ozaki_residues
     from dpnegf_b200.scf import ScfLoop, ozaki_weights
     from dpnegf_b200.surface_green import LeadArena, LeadBlocks, self_energies
     b, L, iters = 512, 40, 10
-    dev = workload.random_device(b, L, seed=512)
+    devs = [workload.random_device(b, L, seed=512 + k) for k in range(nk)]
     kBT, mu_L, vL, vR = 0.025, 0.0, 0.15, -0.15
-    poles, res = ozaki_residues(64)
+    poles, res = ozaki_residues(16)
     fL = lambda x: 1.0 / (1.0 + torch.exp((x - (mu_L - vL)) / kBT))
     fR = lambda x: 1.0 / (1.0 + torch.exp((x - (mu_L - vR)) / kBT))
-    z, c, w = ozaki_weights(poles.numpy(), res.numpy(), 1e6, 231, kBT, mu_L, vL=vL, vR=vR, fermi_L=fL,
+    z, c, w = ozaki_weights(poles.numpy(), res.numpy(), 1e6, 20, kBT, mu_L, vL=vL, vR=vR, fermi_L=fL,
                             fermi_R=fR)
     nE = len(z)
     lb = lambda ld: LeadBlocks(ld.hL, ld.hLL, ld.sL, ld.sLL, ld.hDL, ld.sDL)
-    arena = LeadArena([lb(dev.lead_L), lb(dev.lead_R)])
-    a, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    a.record()
-    ls = self_energies(arena, np.repeat([0, 1], nE), np.tile(z, 2), ETA_LEAD_SYNTH)
-    b_.record()
-    torch.cuda.synchronize()
-    t_lead = a.elapsed_time(b_)
-    seL, seR = torch.stack(ls.sigma[:nE]), torch.stack(ls.sigma[nE:])
-    geom = rgf_plan.Geometry([rgf_plan.DeviceBlocks(dev.hd, dev.hu, dev.hl, dev.sd, dev.su, dev.sl)])
+    arena = LeadArena([lb(ld) for d in devs for ld in (d.lead_L, d.lead_R)])
+    ls, t_lead = _timed(torch, lambda: self_energies(arena, np.repeat(np.arange(2 * nk), nE), np.tile(z, 2 * nk),
+                                                     ETA_LEAD_SYNTH))
+    sig = [torch.stack(ls.sigma[i * nE:(i + 1) * nE]) for i in range(2 * nk)]
+    del arena
+    geom = rgf_plan.Geometry([rgf_plan.DeviceBlocks(d.hd, d.hu, d.hl, d.sd, d.su, d.sl) for d in devs])
+    del devs
     out, ms = {}, {}
     for prec in ("fp64", "mixed"):
-        loop = ScfLoop(geom, seL, seR, z, c, w, alpha=0.5, mix=0.3, eta=1e-5, precision=prec, use_graph=True)
+        loop = ScfLoop(geom, sig[0::2], sig[1::2], z, c, w, alpha=0.5, mix=0.3, eta=1e-5, precision=prec,
+                       use_graph=True)
         loop.run(2)  # iteration 0 (sets n0) and iteration 1 (eager warm-up + graph capture), untimed
-        a, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        a.record()
-        V, n = loop.run(2 + iters)
-        b_.record()
-        torch.cuda.synchronize()
-        ms[prec] = a.elapsed_time(b_)
+        (V, n), ms[prec] = _timed(torch, lambda: loop.run(2 + iters))
         out[prec] = (V.clone(), n.clone())
         loop.restore()
-    pts = nE * iters  # one sweep over every energy per replayed iteration
+        del loop
+    pts = nk * nE * iters  # one sweep over every (k, energy) item per replayed iteration
     ach = 72.0 * b ** 3 * L * pts / (ms["fp64"] * 1e-3) / 1e12
     rel = lambda x, y: float((x - y).abs().max() / max(float(y.abs().max()), 1e-300))
-    return {"b": b, "L": L, "energies": nE, "iterations": iters,
-            "lead_decimation": {"items": 2 * nE, "seconds": t_lead * 1e-3, "n": b,
+    return {"b": b, "L": L, "k_points": nk, "energies_per_k": nE, "iterations": iters,
+            "lead_decimation": {"items": 2 * nk * nE, "seconds": t_lead * 1e-3, "n": b,
                                 "mean_iters": float(ls.iters.mean()),
                                 "tflops_algorithmic": float(_ls_flops(float(b), ls.iters.astype(np.float64)).sum())
                                 / (t_lead * 1e-3) / 1e12},
@@ -473,9 +468,9 @@ def scf_leg(torch, peak):
                       "speedup_vs_fp64": ms["fp64"] / ms["mixed"],
                       "n_rel_err_vs_fp64": rel(out["mixed"][1], out["fp64"][1]),
                       "V_rel_err_vs_fp64": rel(out["mixed"][0], out["fp64"][0])},
-            "note": "energy points = energies x timed iterations; iterations 0-1 (equilibrium n0, graph "
-                    "capture) untimed, then graph replays with the density reduction and potential update, "
-                    "CUDA events around them; " + ETA_LEAD_NOTE}
+            "note": "energy points = k-points x energies x timed iterations; iterations 0-1 (equilibrium n0, "
+                    "graph capture) untimed, then graph replays with the k-summed density reduction and the "
+                    "potential update, CUDA events around them; " + ETA_LEAD_NOTE}
 
 
 def traffic_per_point(b, L):

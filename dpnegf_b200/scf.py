@@ -2,9 +2,9 @@
 
 One iteration of the loop:
 
-  H_qq  <- H0_qq + diag(V_q)                       (in the packed H/S arena)
-  sweep over every energy item                      (one persistent launch)
-  n_i    = Re sum_e c_e diag(G(z_e))_i + sum_e w_e diag(G_qN Gamma_R G_qN^H)(x_e)_i
+  H_qq(k) <- H0_qq(k) + diag(V_q)                  (every k-point, in the packed H/S arena)
+  sweep over every (k, energy) item                 (one persistent launch)
+  n_i    = sum_k wk [Re sum_e c_e diag(G_k(z_e))_i + sum_e w_e diag(G_qN Gamma_R G_qN^H)_k(x_e)_i]
   V      <- V + mix * (alpha * (n - n0) - V)        (damped onsite shifts)
 
 with n0 the equilibrium density of the unshifted device, so the charge
@@ -51,37 +51,54 @@ def ozaki_weights(poles, residues, R, n_gauss, kBT, mu_L, mu_D=0.0, vL=0.0, vR=0
 
 
 class ScfLoop:
-    """Damped onsite-potential SCF of one BTD device around a captured sweep.
+    """Damped onsite-potential SCF of a BTD device around a captured sweep.
 
-    ``se_left`` / ``se_right`` are the lead self-energies at every energy of
-    ``z`` ([B, n, n], e.g. from ``surface_green.self_energies``); ``z, c, w``
-    from ``ozaki_weights``.  ``alpha`` is the onsite response (eV per electron)
-    and ``mix`` the damping.  ``precision`` selects the FP64 or the mixed sweep.
+    ``geometry`` holds the device at one or more k-points (one
+    ``DeviceBlocks`` per k, the same orbitals in each); ``se_left`` /
+    ``se_right`` are the lead self-energies at every energy of ``z``
+    ([B, n, n], e.g. from ``surface_green.self_energies``), or one such stack
+    per k-point.  The density is the ``wk``-weighted sum of the k-point
+    densities (equal weights by default), as the runner sums k contributions
+    (runner/NEGF.py:904-906), and the one potential shifts every k-point's
+    onsite blocks; every (k, energy) item runs in the same launch.  ``z, c, w``
+    from ``ozaki_weights``.  ``alpha`` is the onsite response (eV per
+    electron) and ``mix`` the damping.  ``precision`` selects the FP64 or the
+    mixed sweep.
     """
 
     def __init__(self, geometry: rgf_plan.Geometry, se_left, se_right, z, c, w, alpha=0.5, mix=0.3, eta=0.0,
-                 E_ref=0.0, precision="fp64", use_graph=True):
-        if len(geometry.devs) != 1:
-            raise ValueError("ScfLoop runs one device")
+                 E_ref=0.0, precision="fp64", use_graph=True, wk=None):
+        nk = len(geometry.devs)
+        if not isinstance(se_left, (list, tuple)):
+            se_left, se_right = [se_left], [se_right]
+        if len(se_left) != nk or len(se_right) != nk:
+            raise ValueError(f"one left and one right self-energy stack per k-point ({nk})")
+        if len({int(d["n_orb"]) for d in geometry.devs}) != 1:
+            raise ValueError("every k-point must carry the same orbitals")
+        wk = np.full(nk, 1.0 / nk) if wk is None else np.asarray(wk, dtype=np.float64).reshape(-1)
+        if len(wk) != nk:
+            raise ValueError(f"{len(wk)} k weights for {nk} k-points")
         self.geom = geometry
         dev = geometry.device
-        K = int(geometry.devs[0]["n_blocks"])
         idx = []
-        for q in range(K):
-            b = geometry.blocks[q]
-            n = int(b["n"])
-            idx.append(int(b["hd"]) + np.arange(n) * (n + 1))
+        for d in geometry.devs:
+            for q in range(int(d["blk0"]), int(d["blk0"]) + int(d["n_blocks"])):
+                b = geometry.blocks[q]
+                n = int(b["n"])
+                idx.append(int(b["hd"]) + np.arange(n) * (n + 1))
         self.diag_idx = torch.as_tensor(np.concatenate(idx), device=dev)
         self.h0 = geometry.hs[self.diag_idx].clone()
+        self.nk = nk
         self.n_orb = int(geometry.devs[0]["n_orb"])
         self.B = len(z)
+        self.wk = torch.as_tensor(wk, dtype=torch.float64, device=dev).reshape(nk, 1)
         self.c = torch.as_tensor(np.asarray(c), dtype=torch.complex128, device=dev).reshape(-1, 1)
         self.w = torch.as_tensor(np.asarray(w), dtype=torch.float64, device=dev).reshape(-1, 1)
         self.bias = bool(np.any(np.asarray(w) != 0))
         self.alpha, self.mix = float(alpha), float(mix)
         E = torch.as_tensor(np.asarray(z), dtype=torch.complex128, device=dev)
-        self.plan = rgf_plan.run(geometry, [E], [se_left], [se_right], eta=eta, E_ref=E_ref, outputs=(),
-                                 orb_g=True, orb_ar=self.bias, precision=precision, defer=True)
+        self.plan = rgf_plan.run(geometry, [E] * nk, list(se_left), list(se_right), eta=eta, E_ref=E_ref,
+                                 outputs=(), orb_g=True, orb_ar=self.bias, precision=precision, defer=True)
         self.V = torch.zeros(self.n_orb, dtype=torch.float64, device=dev)
         self.n = torch.zeros(self.n_orb, dtype=torch.float64, device=dev)
         self.n0: Optional[torch.Tensor] = None
@@ -91,16 +108,16 @@ class ScfLoop:
 
     def _density(self, equilibrium_only=False):
         r = self.plan.result
-        n = (self.c * r.orb_g.view(self.B, self.n_orb)).real.sum(0)
+        n = (self.c * r.orb_g.view(self.nk, self.B, self.n_orb)).real.sum(1)
         if self.bias and not equilibrium_only:
-            n = n + (self.w * r.orb_ar.view(self.B, self.n_orb)).sum(0)
-        return n
+            n = n + (self.w * r.orb_ar.view(self.nk, self.B, self.n_orb)).sum(1)
+        return (self.wk * n).sum(0)
 
     def _update(self):
         self.V.add_(self.mix * (self.alpha * (self.n - self.n0) - self.V))
 
     def _body(self):
-        self.geom.hs.index_copy_(0, self.diag_idx, self.h0 + self.V.to(torch.complex128))
+        self.geom.hs.index_copy_(0, self.diag_idx, self.h0 + self.V.to(torch.complex128).repeat(self.nk))
         self.plan.launch()
         self.n.copy_(self._density())
         self._update()
@@ -108,7 +125,7 @@ class ScfLoop:
     def step(self):
         """One SCF iteration; returns the density of that iteration's potential."""
         if self.n0 is None:  # iteration 0: unshifted device, eager, sets n0
-            self.geom.hs.index_copy_(0, self.diag_idx, self.h0 + self.V.to(torch.complex128))
+            self.geom.hs.index_copy_(0, self.diag_idx, self.h0 + self.V.to(torch.complex128).repeat(self.nk))
             self.plan.launch()
             self.plan.check()
             self.n0 = self._density(equilibrium_only=True).clone()

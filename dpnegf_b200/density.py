@@ -279,10 +279,13 @@ class Fiori(Density):
         gn = a_L * fL + a_R * fR
         gp = a_L + a_R - gn
         norbs = [int(x) for x in device_atom_norbs]
+        if sum(norbs) != g.shape[1]:
+            raise ValueError(f"device_atom_norbs covers {sum(norbs)} orbitals, the device has {g.shape[1]}")
         atom_of_orb = torch.as_tensor(np.repeat(np.arange(len(norbs)), norbs), device=dev)
         gn_atom = torch.zeros(B, len(norbs), dtype=gn.dtype, device=dev).index_add_(1, atom_of_orb, gn)
         gp_atom = torch.zeros(B, len(norbs), dtype=gp.dtype, device=dev).index_add_(1, atom_of_orb, gp)
-        Ei = torch.as_tensor(-1 * potential_at_atom).to(dev).reshape(1, -1)
+        # -potential per atom (a list is taken as values, not repeated as -1 * list would)
+        Ei = -torch.as_tensor(potential_at_atom, dtype=torch.float64).to(dev).reshape(1, -1)
         pre = torch.as_tensor(self.pre_factor).to(dev)
         c_e = (pre * 2 * (-1) / 2 / torch.pi).reshape(B, 1)
         c_h = (pre * 2 * 1 / 2 / torch.pi).reshape(B, 1)

@@ -246,3 +246,22 @@ def test_block_inverse_matches_oracle(dims, B):
                            [x.numpy() for x in dev.sl])
     np.testing.assert_allclose(res.trans.cpu().numpy(), T_ref, rtol=1e-10, atol=1e-12)
     np.testing.assert_allclose(res.dos.cpu().numpy(), D_ref, rtol=1e-10, atol=1e-12)
+
+
+def test_empty_energy_batch_gives_empty_blocks():
+    """An empty energy batch returns empty [0, n, m] blocks (the shapes the reference's
+    recursive_gf returns for a [0] energy tensor) and launches nothing."""
+    from dpnegf_b200 import rgf_plan, workload
+    from dpnegf_b200.recursive_green_cal import recursive_gf
+    dims = [4, 5, 4]
+    dev = workload.random_device(0, 0, seed=1, block_dims=dims)
+    E = torch.zeros(0, dtype=torch.complex128, device="cuda")
+    se = torch.zeros(0, 4, 4, dtype=torch.complex128, device="cuda")
+    ans = recursive_gf(E, _cu(dev.hl), _cu(dev.hd), _cu(dev.hu), _cu(dev.sd), _cu(dev.su), _cu(dev.sl), se, se,
+                       eta=1e-5, need_gr_lc=True)
+    assert tuple(ans[0].shape) == (0, 4, 4)
+    assert [tuple(x.shape) for x in ans[1]] == [(0, 4, 4), (0, 5, 4), (0, 4, 4)]
+    assert [tuple(x.shape) for x in ans[2]] == [(0, 4, 4), (0, 5, 5), (0, 4, 4)]
+    geom = rgf_plan.Geometry([rgf_plan.DeviceBlocks(dev.hd, dev.hu, dev.hl, dev.sd, dev.su, dev.sl)])
+    res = rgf_plan.run(geom, [E], [se], [se], eta=1e-5, outputs=(), trans=True, dos=True)
+    assert res.trans.numel() == 0 and res.dos.numel() == 0

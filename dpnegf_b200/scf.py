@@ -23,6 +23,7 @@ from typing import Optional
 
 import numpy as np
 import torch
+import torch.distributed as dist
 
 from . import rgf_plan
 from .negf_utils import gauss_xw
@@ -64,10 +65,18 @@ class ScfLoop:
     from ``ozaki_weights``.  ``alpha`` is the onsite response (eV per
     electron) and ``mix`` the damping.  ``precision`` selects the FP64 or the
     mixed sweep.
+
+    Over several ranks (``group``, or the default process group when one is
+    initialised with more than one rank) each rank passes its own k-points and
+    their weights; the k-summed density is all-reduced once per iteration
+    (one vector of n_orb values), outside the captured graph, and every rank
+    then applies the same potential update.  ``plan``: a deferred plan for
+    ``geometry`` at ``z`` with per-orbital outputs (``rgf_plan.run(...,
+    orb_g=True, orb_ar=bias, defer=True)``), built here when omitted.
     """
 
     def __init__(self, geometry: rgf_plan.Geometry, se_left, se_right, z, c, w, alpha=0.5, mix=0.3, eta=0.0,
-                 E_ref=0.0, precision="fp64", use_graph=True, wk=None):
+                 E_ref=0.0, precision="fp64", use_graph=True, wk=None, group=None, plan=None):
         nk = len(geometry.devs)
         if not isinstance(se_left, (list, tuple)):
             se_left, se_right = [se_left], [se_right]
@@ -96,9 +105,13 @@ class ScfLoop:
         self.w = torch.as_tensor(np.asarray(w), dtype=torch.float64, device=dev).reshape(-1, 1)
         self.bias = bool(np.any(np.asarray(w) != 0))
         self.alpha, self.mix = float(alpha), float(mix)
-        E = torch.as_tensor(np.asarray(z), dtype=torch.complex128, device=dev)
-        self.plan = rgf_plan.run(geometry, [E] * nk, list(se_left), list(se_right), eta=eta, E_ref=E_ref,
-                                 outputs=(), orb_g=True, orb_ar=self.bias, precision=precision, defer=True)
+        self.group = group
+        self.world = dist.get_world_size(group) if dist.is_available() and dist.is_initialized() else 1
+        if plan is None:
+            E = torch.as_tensor(np.asarray(z), dtype=torch.complex128, device=dev)
+            plan = rgf_plan.run(geometry, [E] * nk, list(se_left), list(se_right), eta=eta, E_ref=E_ref,
+                                outputs=(), orb_g=True, orb_ar=self.bias, precision=precision, defer=True)
+        self.plan = plan
         self.V = torch.zeros(self.n_orb, dtype=torch.float64, device=dev)
         self.n = torch.zeros(self.n_orb, dtype=torch.float64, device=dev)
         self.n0: Optional[torch.Tensor] = None
@@ -116,11 +129,25 @@ class ScfLoop:
     def _update(self):
         self.V.add_(self.mix * (self.alpha * (self.n - self.n0) - self.V))
 
+    def _sum_ranks(self, x):
+        if self.world > 1:
+            dist.all_reduce(x, op=dist.ReduceOp.SUM, group=self.group)
+        return x
+
     def _body(self):
+        """Shift, sweep and this rank's density; the update too when one rank holds every k-point
+        (then the whole iteration is one graph)."""
         self.geom.hs.index_copy_(0, self.diag_idx, self.h0 + self.V.to(torch.complex128).repeat(self.nk))
         self.plan.launch()
         self.n.copy_(self._density())
-        self._update()
+        if self.world == 1:
+            self._update()
+
+    def _finish(self):
+        """Over several ranks: the density summed over every rank's k-points, then the update."""
+        if self.world > 1:
+            self._sum_ranks(self.n)
+            self._update()
 
     def step(self):
         """One SCF iteration; returns the density of that iteration's potential."""
@@ -128,8 +155,8 @@ class ScfLoop:
             self.geom.hs.index_copy_(0, self.diag_idx, self.h0 + self.V.to(torch.complex128).repeat(self.nk))
             self.plan.launch()
             self.plan.check()
-            self.n0 = self._density(equilibrium_only=True).clone()
-            self.n.copy_(self._density())
+            self.n0 = self._sum_ranks(self._density(equilibrium_only=True).clone())
+            self.n.copy_(self._sum_ranks(self._density()))
             self._update()
             self.iterations = 1
             return self.n
@@ -139,6 +166,7 @@ class ScfLoop:
             with torch.cuda.stream(s):
                 self._body()  # eager warm-up of the body on a side stream (also iteration 1)
             torch.cuda.current_stream().wait_stream(s)
+            self._finish()
             self.plan.check()
             self.graph = torch.cuda.CUDAGraph()
             with torch.cuda.graph(self.graph, capture_error_mode="relaxed"):
@@ -149,13 +177,15 @@ class ScfLoop:
             self.graph.replay()
         else:
             self._body()
+        self._finish()
         self.iterations += 1
         return self.n
 
     def run(self, iterations=10):
         for _ in range(iterations - self.iterations):
             self.step()
-        torch.cuda.current_stream().synchronize()
+        if self.geom.device.type == "cuda":
+            torch.cuda.current_stream().synchronize()
         self.plan.check()
         return self.V, self.n
 

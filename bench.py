@@ -56,6 +56,8 @@ def parse():
                          "'leads' (its lead decimation alone, --lead-devices devices) and 'scf' (b=512 SCF "
                          "loop captured as a CUDA graph); not in the default run")
     ap.add_argument("--lead-devices", type=int, default=128, help="devices whose leads the 'leads' leg decimates")
+    ap.add_argument("--uneven-precisions", default="fp64,mixed,mixed_refined",
+                    help="runs of the 'uneven' leg besides FP64: mixed, mixed_refined")
     ap.add_argument("--inverse", default=None, choices=["gj", "block"],
                     help="Schur-complement inverse: pivoted Gauss-Jordan or recursive 2x2 blocks "
                          "(default: the autotuned scheme, else block)")
@@ -375,7 +377,7 @@ def leads_leg(torch, peak, n_devices=128, seed=2024):
             "note": ETA_LEAD_NOTE}
 
 
-def uneven_leg(torch, n_devices=128, seed=2024):
+def uneven_leg(torch, n_devices=128, seed=2024, precisions=("fp64", "mixed", "mixed_refined")):
     """The uneven batch (``_uneven_inputs``): every lead at every energy in one decimation launch,
     every (device, energy) item in one persistent sweep (Ozaki.uneven_batch).  FP64, mixed, and
     mixed + FP64-residual refinement, the mixed runs checked against FP64; the decimation phase
@@ -394,7 +396,8 @@ def uneven_leg(torch, n_devices=128, seed=2024):
                                           np.tile(z, 2 * n_devices), ETA_LEAD_SYNTH))[1]
     del arena
     out, ms = {}, {}
-    for tag, prec, refine in (("fp64", "fp64", False), ("mixed", "mixed", False), ("mixed_refined", "mixed", True)):
+    runs = (("fp64", "fp64", False), ("mixed", "mixed", False), ("mixed_refined", "mixed", True))
+    for tag, prec, refine in (r for r in runs if r[0] == "fp64" or r[0] in precisions):
         kw = dict(vL=vL, vR=vR, fermi_L=fL, fermi_R=fR, eta_lead=ETA_LEAD_SYNTH, eta_device=1e-5, precision=prec,
                   refine=refine)
         out[tag], ms[tag] = timed(lambda: oz.uneven_batch(devs, leads, kBT, mu_L, **kw))
@@ -404,7 +407,7 @@ def uneven_leg(torch, n_devices=128, seed=2024):
            "lead_decimation": {"items": 2 * items, "seconds": ms_lead * 1e-3},
            "fp64": {"value": items / (ms["fp64"] * 1e-3), "unit": "items/s", "seconds": ms["fp64"] * 1e-3,
                     "sweep_tflops_algorithmic": work * nE / ((ms["fp64"] - ms_lead) * 1e-3) / 1e12}}
-    for tag in ("mixed", "mixed_refined"):
+    for tag in (t for t in ("mixed", "mixed_refined") if t in out):
         res[tag] = {"value": items / (ms[tag] * 1e-3), "unit": "items/s", "seconds": ms[tag] * 1e-3,
                     "density_rel_err_vs_fp64": max(rel(m["n_eq"] + m["n_neq"], f["n_eq"] + f["n_neq"])
                                                    for m, f in zip(out[tag], out["fp64"])),
@@ -731,7 +734,7 @@ def main():
         if "leads" in wanted:
             extra["config3_leads"] = leads_leg(torch, peak, n_devices=args.lead_devices)
         if "uneven" in wanted:
-            extra["config3_uneven"] = uneven_leg(torch)
+            extra["config3_uneven"] = uneven_leg(torch, precisions=args.uneven_precisions.split(","))
         if "scf" in wanted:
             extra["config5_scf"] = scf_leg(torch, peak)
 

@@ -56,6 +56,7 @@ def parse():
                          "'leads' (its lead decimation alone, --lead-devices devices) and 'scf' (b=512 SCF "
                          "loop captured as a CUDA graph); not in the default run")
     ap.add_argument("--lead-devices", type=int, default=128, help="devices whose leads the 'leads' leg decimates")
+    ap.add_argument("--uneven-devices", type=int, default=128, help="devices of the 'uneven' leg")
     ap.add_argument("--uneven-precisions", default="fp64,mixed,mixed_refined",
                     help="runs of the 'uneven' leg besides FP64: mixed, mixed_refined")
     ap.add_argument("--inverse", default=None, choices=["gj", "block"],
@@ -734,7 +735,8 @@ def main():
         if "leads" in wanted:
             extra["config3_leads"] = leads_leg(torch, peak, n_devices=args.lead_devices)
         if "uneven" in wanted:
-            extra["config3_uneven"] = uneven_leg(torch, precisions=args.uneven_precisions.split(","))
+            extra["config3_uneven"] = uneven_leg(torch, n_devices=args.uneven_devices,
+                                                 precisions=args.uneven_precisions.split(","))
         if "scf" in wanted:
             extra["config5_scf"] = scf_leg(torch, peak)
 

@@ -82,8 +82,9 @@ class Ozaki(Density):
         vL, vR = float(deviceprop.lead_L.voltage), float(deviceprop.lead_R.voltage)
         if abs(vL - vR) > 1e-14:
             xl, xu = min(vL, vR) - 8 * kBT, max(vL, vR) + 8 * kBT
-            xs, wlg = gauss_xw(xl=torch.scalar_tensor(xl, dtype=torch.float64),
-                               xu=torch.scalar_tensor(xu, dtype=torch.float64), n=self.n_gauss)
+            # as the reference (density.py:186): limits from torch.scalar_tensor (the default dtype,
+            # float32), so the nodes, weights and Fermi factors are float32
+            xs, wlg = gauss_xw(xl=torch.scalar_tensor(xl), xu=torch.scalar_tensor(xu), n=self.n_gauss)
             Gr = self._green_first_block(deviceprop, kpoint, xs.to(torch.complex128), eta_lead, eta_device,
                                          None, block_tridiagonal)
             gam = deviceprop.lead_R.gamma.to(Gr.device)
@@ -92,9 +93,10 @@ class Ozaki(Density):
             GR = torch.zeros(gam.shape[0], n0, n0, dtype=torch.complex128, device=Gr.device)
             GR[:, n0 - cr:, n0 - cr:] = gam[:, gam.shape[-2] - cr:, gam.shape[-1] - cr:]
             A = (Gr @ GR @ Gr.mH).real
-            e = xs.to(Gr.device)
-            df = (deviceprop.lead_R.fermi_dirac(e + mu_D) - deviceprop.lead_L.fermi_dirac(e + mu_D)).real
-            DM_neq = (wlg.to(Gr.device).reshape(-1, 1, 1) * A * df.reshape(-1, 1, 1)).sum(0)
+            # f_R - f_L per node on 0-d host tensors, the reference's arithmetic (density.py:192)
+            df = torch.stack([torch.as_tensor(deviceprop.lead_R.fermi_dirac(x + mu_D)
+                                              - deviceprop.lead_L.fermi_dirac(x + mu_D)).real.cpu() for x in xs])
+            DM_neq = (wlg.to(Gr.device).reshape(-1, 1, 1) * (A * df.to(Gr.device).reshape(-1, 1, 1))).sum(0)
         else:
             DM_neq = 0.
         return DM_eq, DM_neq

@@ -95,6 +95,15 @@ def gauss_xw(xl, xu, n):
     return x * (0.5 * (xu - xl)) + 0.5 * (xu + xl), w * 0.5 * (xu - xl)
 
 
+def gauss_xw_f32(xl, xu, n):
+    """``gauss_xw`` as ``Ozaki.integrate`` evaluates it (negf/density.py:186, negf_utils.py:153-158):
+    the limits come from ``torch.scalar_tensor`` (float32), so nodes and weights are float32."""
+    x, w = np.polynomial.legendre.leggauss(n)
+    xl32, xu32 = np.float32(xl), np.float32(xu)
+    half = np.float32(0.5) * (xu32 - xl32)
+    return x.astype(np.float32) * half + np.float32(0.5) * (xu32 + xl32), w.astype(np.float32) * half
+
+
 def ozaki_density(gf, mu_L, mu_D, kBT, R, M_cut, n_gauss, vL, vR, fermi_L, fermi_R, gamma_R_fn):
     """Restatement of ``Ozaki.integrate`` (negf/density.py:143-199) with explicit mu.
 
@@ -107,7 +116,9 @@ def ozaki_density(gf, mu_L, mu_D, kBT, R, M_cut, n_gauss, vL, vR, fermi_L, fermi
     DM_eq = Re[ iR G(iR - mu_D) - sum_p Im(-4 i kT G(z_p) r_p) ],
     z_p = i pole_p kT + mu_L - mu_D;
     DM_neq = sum_i w_i Re[G Gamma_R G^H] (f_R - f_L) at Gauss-Legendre points
-    on [min(vL,vR) - 8kT, max(vL,vR) + 8kT] when the bias is non-zero.
+    on [min(vL,vR) - 8kT, max(vL,vR) + 8kT] when the bias is non-zero; nodes, weights, the Fermi
+    factors at x + mu_D and their difference are float32 there, as the reference forms them
+    (``fermi_L`` / ``fermi_R`` receive a float32 argument).
     """
     poles, res = ozaki_residues(M_cut)
     zp = 1j * poles * kBT + mu_L - mu_D
@@ -117,12 +128,14 @@ def ozaki_density(gf, mu_L, mu_D, kBT, R, M_cut, n_gauss, vL, vR, fermi_L, fermi
     dm_eq = np.real(dm)
     if abs(vL - vR) > 1e-14:
         xl, xu = min(vL, vR) - 8 * kBT, max(vL, vR) + 8 * kBT
-        xs, wl = gauss_xw(xl, xu, n_gauss)
+        xs, wl = gauss_xw_f32(xl, xu, n_gauss)
         dm_neq = 0.0
         for x, w in zip(xs, wl):
-            G = gf(x)
-            a = np.real(G @ gamma_R_fn(x) @ G.conj().T)
-            dm_neq = dm_neq + w * a * (fermi_R(x + mu_D) - fermi_L(x + mu_D))
+            G = gf(complex(x))
+            a = np.real(G @ gamma_R_fn(complex(x)) @ G.conj().T)
+            e = x + np.float32(mu_D)
+            df = np.float32(fermi_R(e)) - np.float32(fermi_L(e))
+            dm_neq = dm_neq + w * (a * df)
     else:
         dm_neq = 0.0
     return dm_eq, dm_neq

@@ -31,7 +31,13 @@ seeded inputs together with the reference's own outputs:
                   so for that case the fake device property asks
                   ``cal_green_function`` for it (``need_gr_lc=True``); the
                   leads serve seeded self-energies per grid energy.  Also the
-                  reference's ``get_subblock_index`` for every atom.
+                  reference's ``get_subblock_index`` for every atom;
+  ozaki_integrate.npz  ``Ozaki.integrate`` (negf/density.py:143-199) on a
+                  single-block device under bias: the reference reads
+                  ``deviceprop.mu`` and ``lead_L.mu``, which its classes never
+                  set, so the fake device property carries them; the leads
+                  compute their self-energies with the reference's own
+                  ``selfEnergy`` (as ``LeadProperty.self_energy_cal`` does).
 The fixtures are small (tens of KB) and are committed; the GPU box never needs
 the reference sources.
 """
@@ -253,6 +259,69 @@ def _fiori_case(dp_mod, dens_mod, name, dims, norbs, block_tridiagonal, integrat
     np.savez_compressed(os.path.join(HERE, f"fiori_{name}.npz"), **d)
 
 
+class _SelfEnergyLead(_FakeLead):
+    """Lead whose ``self_energy`` runs the reference's ``selfEnergy`` on fixed lead blocks, as
+    ``LeadProperty.self_energy_cal`` does for a non-Bloch lead (lead_property.py:305-328)."""
+
+    def __init__(self, sg_mod, blocks, voltage, efermi, kBT):
+        super().__init__(efermi - voltage, kBT)
+        self._sg, self._blocks = sg_mod, blocks
+        self.voltage, self.efermi = voltage, efermi
+
+    def self_energy(self, kpoint, energy, eta_lead=1e-5, save_path=None, **kw):
+        hL, hLL, sL, sLL, hDL, sDL = self._blocks
+        if not isinstance(energy, torch.Tensor):  # as LeadProperty.self_energy (lead_property.py:135-136)
+            energy = torch.tensor(energy)
+        self.se, _ = self._sg.selfEnergy(hL=hL, hLL=hLL, sL=sL, sLL=sLL, ee=energy, hDL=hDL, sDL=sDL,
+                                         etaLead=eta_lead, E_ref=0.0)
+
+
+def _ozaki_integrate_case(dp_mod, dens_mod, sg_mod):
+    from scipy.constants import Boltzmann
+    kBT = Boltzmann * 300 / 1.6021766208e-19
+    dev = workload.random_device(12, 3, seed=3)
+    one = workload.BTDDevice([dev.hd[1]], [], [], [dev.sd[1]], [], [])
+    lead_blocks = {}
+    for tab, ld in (("lead_L", dev.lead_L), ("lead_R", dev.lead_R)):
+        lead_blocks[tab] = (ld.hL, ld.hLL, ld.sL, ld.sLL, ld.hDL, ld.sDL)
+    dp = dp_mod.DeviceProperty.__new__(dp_mod.DeviceProperty)
+    dp.greenfuncs = 0
+    dp.hamiltonian = _FakeHamiltonian(one)
+    dp.structure = None
+    dp.results_path = "/nonexistent-negf-results"
+    dp.cdtype = torch.complex128
+    dp.rgf_device = "cpu"
+    dp.kBT = kBT
+    dp.e_T = 300.0
+    dp.chemiPot = None
+    dp.E_ref = 0.0
+    dp.kpoint = None
+    dp.newK_flag = None
+    dp.newV_flag = None
+    dp.lead_L = _SelfEnergyLead(sg_mod, lead_blocks["lead_L"], 0.1, 0.0, kBT)
+    dp.lead_R = _SelfEnergyLead(sg_mod, lead_blocks["lead_R"], -0.1, 0.0, kBT)
+    dp.mu = 0.0                                   # mu_D: the device reference level
+    dp.lead_L.mu = dp.lead_L.chemiPot_lead        # mu_L: the left lead's chemical potential
+    oz = dens_mod.Ozaki(R=1e6, M_cut=20, n_gauss=6)
+    DM_eq, DM_neq = oz.integrate(dp, kpoint=[0.0, 0.0, 0.0], eta_lead=1e-5, eta_device=0.0, block_tridiagonal=False)
+    d = {}
+    _put(d, "hd", one.hd)
+    _put(d, "sd", one.sd)
+    for tab in ("lead_L", "lead_R"):
+        for name, t in zip(("hL", "hLL", "sL", "sLL", "hDL", "sDL"), lead_blocks[tab]):
+            _put(d, f"{tab}/{name}", t)
+    _put(d, "kBT", np.array(kBT))
+    _put(d, "vL", np.array(0.1))
+    _put(d, "vR", np.array(-0.1))
+    _put(d, "mu_L", np.array(dp.lead_L.mu))
+    _put(d, "R", np.array(1e6))
+    _put(d, "M_cut", np.array(20))
+    _put(d, "n_gauss", np.array(6))
+    _put(d, "out/DM_eq", DM_eq)
+    _put(d, "out/DM_neq", DM_neq)
+    np.savez_compressed(os.path.join(HERE, "ozaki_integrate.npz"), **d)
+
+
 def _lopez_cases(sg_mod):
     d = {}
     chain = workload.chain_device(L=4)
@@ -385,7 +454,7 @@ def _adjoint_dos_case(rgf_mod, name, dims, B, seed, with_t, eta=1e-5):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default=ref_import.DEFAULT_REF_ROOT)
-    ap.add_argument("--only", default=None, help="regenerate one family: rgf, devprop, lopez, ozaki, adjoint, fiori")
+    ap.add_argument("--only", default=None, help="regenerate one family: rgf, devprop, lopez, ozaki, adjoint, fiori, ozaki_integrate")
     args = ap.parse_args()
     torch.set_num_threads(1)  # the container's threaded batched zgesv can hang
     rgf_mod = ref_import.load("recursive_green_cal", args.ref_root)
@@ -419,6 +488,8 @@ def main():
         _adjoint_dos_case(rgf_mod, "nonuniform", [6, 9, 5, 7], 3, seed=24, with_t=False)
         _adjoint_dos_case(rgf_mod, "uniform_with_t", [10] * 5, 2, seed=25, with_t=True)
         _adjoint_dos_case(rgf_mod, "single_block", [8], 2, seed=26, with_t=False)
+    if want("ozaki_integrate"):
+        _ozaki_integrate_case(dp_mod, dens_mod, sg_mod)
     if want("fiori"):
         _fiori_case(dp_mod, dens_mod, "dense_direct", [9], [2, 3, 4], False, "direct", seed=31, nL=3, nR=4)
         _fiori_case(dp_mod, dens_mod, "dense_gauss", [9], [2, 3, 4], False, "gauss", seed=32, nL=3, nR=4)

@@ -166,8 +166,9 @@ def test_ozaki_equilibrium_density_matches_oracle():
         s = se(lR, x, 1e-5)
         return 1j * (s - s.conj().T)
 
-    fL = lambda x: float(lL.fermi_dirac(torch.as_tensor(float(np.real(x)), dtype=torch.float64)))
-    fR = lambda x: float(lR.fermi_dirac(torch.as_tensor(float(np.real(x)), dtype=torch.float64)))
+    # the oracle passes float32 arguments (the reference's float32 bias-window quadrature)
+    fL = lambda x: float(lL.fermi_dirac(torch.tensor(x)))
+    fR = lambda x: float(lR.fermi_dirac(torch.tensor(x)))
     ref_eq, ref_neq = lead_oracle.ozaki_density(gf, lL.chemiPot_lead, 0.0, kBT, 1e6, 20, 6, lL.voltage,
                                                 lR.voltage, fL, fR, gamma_R)
     assert _rel(DM_eq, ref_eq) < 1e-9
@@ -388,3 +389,41 @@ def test_fiori_free_charge_matches_reference_fixture(case, dirichlet):
     for a in range(len(norbs)):
         bl, s0, s1 = fi.get_subblock_index(dims, a, norbs)
         assert list(bl) + [s0, s1] == [int(x) for x in g[f"out/subblock/{a}"]]
+
+
+class _FixedLeadHamiltonian(FakeHamiltonian):
+    """Serves the fixture's lead blocks unshifted by the lead voltage, as the reference run did."""
+
+    def get_hs_lead(self, kpoint, tab, v):
+        L = self.leads[tab]
+        return (L.hL, L.hLL, L.hDL, L.sL, L.sLL, L.sDL)
+
+
+def test_ozaki_integrate_matches_reference_fixture():
+    """Ozaki.integrate (poles and bias window each in one lead launch per lead and one RGF launch)
+    against the reference's own Ozaki.integrate on the same single-block device under +-0.1 V:
+    DM_eq and DM_neq within 1e-9 relative (float32 bias-window quadrature as the reference)."""
+    from types import SimpleNamespace
+    from dpnegf_b200 import workload
+    from dpnegf_b200.density import Ozaki
+    from dpnegf_b200.device_property import DeviceProperty
+    from dpnegf_b200.lead_property import LeadProperty
+    g = Golden("ozaki_integrate")
+    one = workload.BTDDevice([torch.as_tensor(x) for x in g["hd"]], [], [], [torch.as_tensor(x) for x in g["sd"]],
+                             [], [])
+    n = one.block_dims[0]
+    leads = {t: SimpleNamespace(**{k: torch.as_tensor(g[f"{t}/{k}"]) for k in ("hL", "hLL", "sL", "sLL", "hDL", "sDL")})
+             for t in ("lead_L", "lead_R")}
+    ham = _FixedLeadHamiltonian(one, [1] * n, leads=leads, subblocks=[n])
+    dp = DeviceProperty(ham, None, "", e_T=300, E_ref=0.0)
+    assert dp.kBT == float(g["kBT"])
+    lL = LeadProperty("lead_L", ham, None, "", voltage=float(g["vL"]), efermi=0.0)
+    lR = LeadProperty("lead_R", ham, None, "", voltage=float(g["vR"]), efermi=0.0)
+    dp.set_leadLR(lL, lR)
+    oz = Ozaki(R=float(g["R"]), M_cut=int(g["M_cut"]), n_gauss=int(g["n_gauss"]))
+    DM_eq, DM_neq = oz.integrate(dp, [0.0, 0.0, 0.0], eta_lead=1e-5, eta_device=0.0, mu=0.0,
+                                 mu_lead=float(g["mu_L"]))
+    print(f"Ozaki.integrate vs reference: DM_eq {_rel(DM_eq, g['out/DM_eq']):.2e}, "
+          f"DM_neq {_rel(DM_neq, g['out/DM_neq']):.2e}")
+    assert _rel(DM_eq, g["out/DM_eq"]) < 1e-9
+    assert _rel(DM_neq, g["out/DM_neq"]) < 1e-9

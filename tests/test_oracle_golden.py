@@ -143,3 +143,31 @@ def test_fiori_subblock_index_matches_reference(case):
     for a in range(len(norbs)):
         bl, s0, s1 = lead_oracle.fiori_subblock_index(dims, a, norbs)
         assert list(bl) + [s0, s1] == [int(x) for x in g[f"out/subblock/{a}"]]
+
+
+def test_ozaki_integrate_matches_reference():
+    """The Ozaki density restatement against the reference's own Ozaki.integrate (single-block device
+    under +-0.1 V, mu set on the fake objects it reads): DM_eq and DM_neq within 1e-10 relative,
+    the bias-window quadrature and Fermi factors in float32 as the reference forms them."""
+    g = Golden("ozaki_integrate")
+    kBT, vL, vR, muL = float(g["kBT"]), float(g["vL"]), float(g["vR"]), float(g["mu_L"])
+    leads = {t: [g[f"{t}/{k}"] for k in ("hL", "hLL", "sL", "sLL", "hDL", "sDL")] for t in ("lead_L", "lead_R")}
+
+    def se(t, z, eta=1e-5):
+        hL, hLL, sL, sLL, hDL, sDL = leads[t]
+        return lead_oracle.self_energy(hL, hLL, sL, sLL, z, hDL, sDL, etaLead=eta, E_ref=0.0)[0]
+
+    def gf(z):
+        return rgf_oracle.rgf(np.array([z]), [], g["hd"], [], g["sd"], [], [], se("lead_L", z)[None],
+                              se("lead_R", z)[None], eta=0.0)["grd"][0][0]
+
+    def gamma_R(x):
+        s = se("lead_R", x)
+        return 1j * (s - s.conj().T)
+
+    fL = lambda x: 1.0 / (1.0 + np.exp((x - (0.0 - vL)) / kBT))
+    fR = lambda x: 1.0 / (1.0 + np.exp((x - (0.0 - vR)) / kBT))
+    eq, neq = lead_oracle.ozaki_density(gf, muL, 0.0, kBT, float(g["R"]), int(g["M_cut"]), int(g["n_gauss"]),
+                                        vL, vR, fL, fR, gamma_R)
+    for got, want in ((eq, g["out/DM_eq"]), (neq, g["out/DM_neq"])):
+        assert np.abs(got - want).max() < 1e-10 * np.abs(want).max()

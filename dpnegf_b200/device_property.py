@@ -234,7 +234,8 @@ class DeviceProperty(object):
         vmin, vmax = emin + 4 * self.kBT, emax - 4 * self.kBT
         vm = 0.5 * (vmin + vmax)
         vmid = vm - vmin
-        vv = torch.linspace(start=0., end=float(vmid), steps=int(vmid / 0.1) + 1, dtype=torch.float64) * 2
+        # the default dtype (float32), as the reference's torch.linspace (device_property.py:362)
+        vv = torch.linspace(start=0., end=float(vmid), steps=int(vmid / 0.1) + 1) * 2
         cc = []
         for dv in vv * 0.5:
             y = (f(energy_grid + efermi, efermi - vm + dv) - f(energy_grid + efermi, efermi - vm - dv)) * tc

@@ -149,9 +149,11 @@ def current_nscf(energy_grid, tc, efermi, kBT):
     vmin, vmax = emin + 4 * kBT, emax - 4 * kBT
     vm = 0.5 * (vmin + vmax)
     vmid = vm - vmin
-    vv = np.linspace(0.0, vmid, int(vmid / 0.1) + 1) * 2
-    cc = [simpson(y=(f(energy_grid + efermi, efermi - vm + dv) - f(energy_grid + efermi, efermi - vm - dv)) * tc,
-                  x=energy_grid) for dv in vv * 0.5]
+    # the bias grid is float32 there (torch.linspace in the default dtype); each half-bias dv enters
+    # the float64 chemical potentials with its float32 value
+    vv = np.linspace(0.0, vmid, int(vmid / 0.1) + 1).astype(np.float32) * np.float32(2)
+    cc = [simpson(y=(f(energy_grid + efermi, efermi - vm + float(dv)) - f(energy_grid + efermi, efermi - vm - float(dv)))
+                  * tc, x=energy_grid) for dv in vv * np.float32(0.5)]
     return vv, np.array(cc)
 
 

@@ -37,7 +37,9 @@ seeded inputs together with the reference's own outputs:
                   ``deviceprop.mu`` and ``lead_L.mu``, which its classes never
                   set, so the fake device property carries them; the leads
                   compute their self-energies with the reference's own
-                  ``selfEnergy`` (as ``LeadProperty.self_energy_cal`` does).
+                  ``selfEnergy`` (as ``LeadProperty.self_energy_cal`` does);
+  current_nscf.npz  ``DeviceProperty._cal_current_nscf_`` (negf/device_property.py:333-371):
+                  the bias grid and Simpson currents for a smooth T(E).
 The fixtures are small (tens of KB) and are committed; the GPU box never needs
 the reference sources.
 """
@@ -322,6 +324,26 @@ def _ozaki_integrate_case(dp_mod, dens_mod, sg_mod):
     np.savez_compressed(os.path.join(HERE, "ozaki_integrate.npz"), **d)
 
 
+def _current_case(dp_mod):
+    from types import SimpleNamespace
+    from scipy.constants import Boltzmann
+    dp = dp_mod.DeviceProperty.__new__(dp_mod.DeviceProperty)
+    dp.kBT = Boltzmann * 300 / 1.6021766208e-19
+    dp.lead_L = SimpleNamespace(efermi=0.1)
+    dp.lead_R = SimpleNamespace(efermi=0.1)
+    E = torch.linspace(-1.0, 1.0, 41, dtype=torch.float64)
+    tc = 1.0 + 0.5 * torch.sin(3 * E) ** 2
+    vv, cc = dp._cal_current_nscf_(E, tc)
+    d = {}
+    _put(d, "energy", E)
+    _put(d, "tc", tc)
+    _put(d, "efermi", np.array(0.1))
+    _put(d, "kBT", np.array(dp.kBT))
+    _put(d, "out/vv", vv)
+    _put(d, "out/cc", np.array([float(c) for c in cc]))
+    np.savez_compressed(os.path.join(HERE, "current_nscf.npz"), **d)
+
+
 def _lopez_cases(sg_mod):
     d = {}
     chain = workload.chain_device(L=4)
@@ -454,7 +476,7 @@ def _adjoint_dos_case(rgf_mod, name, dims, B, seed, with_t, eta=1e-5):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default=ref_import.DEFAULT_REF_ROOT)
-    ap.add_argument("--only", default=None, help="regenerate one family: rgf, devprop, lopez, ozaki, adjoint, fiori, ozaki_integrate")
+    ap.add_argument("--only", default=None, help="regenerate one family: rgf, devprop, lopez, ozaki, adjoint, fiori, ozaki_integrate, current")
     args = ap.parse_args()
     torch.set_num_threads(1)  # the container's threaded batched zgesv can hang
     rgf_mod = ref_import.load("recursive_green_cal", args.ref_root)
@@ -488,6 +510,8 @@ def main():
         _adjoint_dos_case(rgf_mod, "nonuniform", [6, 9, 5, 7], 3, seed=24, with_t=False)
         _adjoint_dos_case(rgf_mod, "uniform_with_t", [10] * 5, 2, seed=25, with_t=True)
         _adjoint_dos_case(rgf_mod, "single_block", [8], 2, seed=26, with_t=False)
+    if want("current"):
+        _current_case(dp_mod)
     if want("ozaki_integrate"):
         _ozaki_integrate_case(dp_mod, dens_mod, sg_mod)
     if want("fiori"):

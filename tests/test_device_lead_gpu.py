@@ -240,6 +240,9 @@ def test_runner_nscf_loop_matches_oracle():
         assert _rel(out["LDOS"][str(k)].sum(-1), np.array(D_ref)) < 1e-9
     assert _rel(out["T_avg"], np.array(T_ref)) < 1e-9
     assert len(out["CURRENT_NSCF"]) == len(out["BIAS_POTENTIAL_NSCF"])
+    vv, cc = lead_oracle.current_nscf(E.numpy(), np.array(T_ref), lL.efermi, lL.kBT)
+    np.testing.assert_array_equal(out["BIAS_POTENTIAL_NSCF"].cpu().numpy(), vv)
+    assert _rel(torch.stack([torch.as_tensor(c) for c in out["CURRENT_NSCF"]]), cc) < 1e-9
 
 
 def test_local_current_matches_reference_loop():

@@ -6,6 +6,7 @@ check the CUDA path.
 """
 import numpy as np
 import pytest
+import torch
 
 from oracle import lead_oracle, rgf_oracle
 from tests.goldens import Golden, rgf_cases
@@ -171,3 +172,23 @@ def test_ozaki_integrate_matches_reference():
                                         vL, vR, fL, fR, gamma_R)
     for got, want in ((eq, g["out/DM_eq"]), (neq, g["out/DM_neq"])):
         assert np.abs(got - want).max() < 1e-10 * np.abs(want).max()
+
+
+def test_current_nscf_matches_reference():
+    """The NSCF I-V restatement and the product's torch version (CPU tensors) against the reference's
+    _cal_current_nscf_: the float32 bias grid exactly, the currents within 1e-12 relative."""
+    from types import SimpleNamespace
+    from dpnegf_b200.device_property import DeviceProperty
+    g = Golden("current_nscf")
+    E, tc, efermi, kBT = g["energy"], g["tc"], float(g["efermi"]), float(g["kBT"])
+    vv, cc = lead_oracle.current_nscf(E, tc, efermi, kBT)
+    np.testing.assert_array_equal(vv, g["out/vv"])
+    assert np.abs(cc - g["out/cc"]).max() < 1e-12 * np.abs(g["out/cc"]).max()
+    dp = DeviceProperty.__new__(DeviceProperty)
+    dp.kBT = kBT
+    dp.lead_L = dp.lead_R = SimpleNamespace(efermi=efermi)
+    v2, c2 = dp._cal_current_nscf_(torch.as_tensor(E), torch.as_tensor(tc))
+    assert v2.dtype == torch.float32
+    np.testing.assert_array_equal(v2.numpy(), g["out/vv"])
+    c2 = np.array([float(c) for c in c2])
+    assert np.abs(c2 - g["out/cc"]).max() < 1e-12 * np.abs(g["out/cc"]).max()

@@ -87,6 +87,17 @@ NEGF_DEV void gemm_ls(cplx* smem, int M, int N, int K, const cplx* A, int64_t ld
 NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, char* smem_raw, double* red) {
   cplx* smem = reinterpret_cast<cplx*>(smem_raw);
   const NegfLead ld = P.leads[it.lead];
+  // every slot buffer holds max_n^2 elements: refuse a lead that would not fit (H_DL products are
+  // nc x b and nc x nc) before touching any memory
+  if (ld.n <= 0 || ld.n > P.max_n || ld.nc < 0 || ld.nc > P.max_n || (ld.nc > 0 && (ld.b <= 0 || ld.b > ld.n))) {
+    if (threadIdx.x == 0) {
+      P.status[it.out] = NEGF_ERR_ARGUMENT;
+      if (P.iters) P.iters[it.out] = 0;
+      if (P.resid) P.resid[it.out] = INFINITY;
+    }
+    __syncthreads();
+    return;
+  }
   const int n = ld.n;
   const int64_t n2 = (int64_t)n * n;
   const size_t mn2 = (size_t)P.max_n * P.max_n;

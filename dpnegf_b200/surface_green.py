@@ -84,6 +84,8 @@ class LeadArena:
                 rec["nc"], rec["b"] = nc, b
                 rec["hdl"], rec["sdl"] = put(ld.hDL), put(sdl)
                 self.shapes.append((n, nc))
+                # the self-energy products are nc x b and nc x nc: slot buffers are sized by max(n, nc)
+                self.max_n = max(self.max_n, nc)
             else:
                 rec["nc"], rec["b"] = 0, n
                 rec["hdl"] = rec["sdl"] = -1
@@ -168,6 +170,8 @@ def raise_for_status(status, resid, E):
             raise RuntimeError("Lopez-scheme not converged.")
         elif s == _lib.NEGF_ERR_SINGULAR:
             raise ArithmeticError(f"Lopez-Sancho: singular matrix at E = {E[i].real:.4f} eV")
+        elif s == _lib.NEGF_ERR_ARGUMENT:
+            raise ValueError(f"Lopez-Sancho: item {i} has a lead larger than the problem's max_n")
 
 
 def selfEnergy(hL, hLL, sL, sLL, ee, hDL=None, sDL=None, etaLead=1e-8, Bulk=False,

@@ -193,7 +193,8 @@ typedef struct NegfLsProblem {
   const NegfLead* leads;    /* device memory */
   const NegfLsItem* items;  /* device memory */
   int32_t n_items;
-  int32_t max_n;
+  int32_t max_n;            /* largest of n and nc over all leads (sizes the slot buffers; an item whose
+                               lead exceeds it gets NEGF_ERR_ARGUMENT as its status and is skipped) */
   const double* arena;      /* complex128 lead blocks */
   int32_t* status;          /* [n_items]: NEGF_OK, NEGF_WARN_LS_CONVERGENCE, NEGF_ERR_LS_* , NEGF_ERR_SINGULAR */
   int32_t* iters;           /* [n_items] decimation steps taken */

@@ -39,7 +39,12 @@ seeded inputs together with the reference's own outputs:
                   compute their self-energies with the reference's own
                   ``selfEnergy`` (as ``LeadProperty.self_energy_cal`` does);
   current_nscf.npz  ``DeviceProperty._cal_current_nscf_`` (negf/device_property.py:333-371):
-                  the bias grid and Simpson currents for a smooth T(E).
+                  the bias grid and Simpson currents for a smooth T(E);
+  lead_property.npz  ``LeadProperty.self_energy`` (negf/lead_property.py:105-158, 266-328):
+                  both leads of a two-block device under a lead voltage, H_DL
+                  trimmed to the edge block by ``HDL_reduced``, Python-float and
+                  complex-tensor energies (a file path that does not exist is
+                  given as ``save_path``, so nothing is read or written).
 The fixtures are small (tens of KB) and are committed; the GPU box never needs
 the reference sources.
 """
@@ -344,6 +349,61 @@ def _current_case(dp_mod):
     np.savez_compressed(os.path.join(HERE, "current_nscf.npz"), **d)
 
 
+class _LeadHamiltonian:
+    """Lead blocks shifted by the lead voltage (H - v S), and the device's sub-block sizes."""
+
+    def __init__(self, blocks, subblocks):
+        self.blocks, self.subblocks = blocks, subblocks
+
+    def get_hs_device(self, kpoint, V=None, block_tridiagonal=True, only_subblocks=False):
+        return self.subblocks
+
+    def get_hs_lead(self, kpoint, tab, v):
+        hL, hLL, hDL, sL, sLL, sDL = self.blocks[tab]
+        return hL - v * sL, hLL - v * sLL, hDL, sL, sLL, sDL
+
+
+def _lead_property_blocks(seed=41, n=4, sub=(5, 7)):
+    """Random non-orthogonal lead layers; H_DL / S_DL nonzero only in the rows of the device block
+    the lead couples to (the first block for lead_L, the last for lead_R)."""
+    gen = torch.Generator().manual_seed(seed)
+    c = lambda *s: torch.complex(torch.randn(*s, generator=gen, dtype=torch.float64),
+                                 torch.randn(*s, generator=gen, dtype=torch.float64))
+    nd = sum(sub)
+    blocks = {}
+    for tab in ("lead_L", "lead_R"):
+        h = c(n, n) * 0.2
+        h = 0.5 * (h + h.mH) + torch.diag(torch.linspace(-1.0, 1.0, n, dtype=torch.float64)).to(torch.complex128)
+        s = torch.eye(n, dtype=torch.complex128) + 0.01 * (lambda x: 0.5 * (x + x.mH))(c(n, n))
+        hLL, sLL = 0.6 * c(n, n) / n ** 0.5, 0.01 * c(n, n) / n ** 0.5
+        hDL, sDL = torch.zeros(nd, n, dtype=torch.complex128), torch.zeros(nd, n, dtype=torch.complex128)
+        rows = slice(0, sub[0]) if tab == "lead_L" else slice(nd - sub[-1], nd)
+        m = sub[0] if tab == "lead_L" else sub[-1]
+        hDL[rows] = 0.5 * c(m, n) / n ** 0.5
+        sDL[rows] = 0.01 * c(m, n) / n ** 0.5
+        blocks[tab] = (h, hLL, hDL, s, sLL, sDL)
+    return blocks, list(sub)
+
+
+def _lead_property_case(lp_mod):
+    blocks, sub = _lead_property_blocks()
+    ham = _LeadHamiltonian(blocks, sub)
+    energies = [-0.3, 0.25, torch.tensor(0.1 + 0.2j, dtype=torch.complex128)]
+    d = {}
+    _put(d, "subblocks", np.array(sub))
+    for tab, v in (("lead_L", 0.05), ("lead_R", -0.05)):
+        for name, t in zip(("hL", "hLL", "hDL", "sL", "sLL", "sDL"), blocks[tab]):
+            _put(d, f"{tab}/{name}", t)
+        _put(d, f"{tab}/voltage", np.array(v))
+        lead = lp_mod.LeadProperty(tab, ham, None, "/nonexistent-negf-results", voltage=v, efermi=0.1)
+        for i, e in enumerate(energies):
+            lead.self_energy(kpoint=[0.0, 0.0, 0.0], energy=e, eta_lead=1e-5,
+                             save_path="/nonexistent-negf-se/self_energy.h5")
+            _put(d, f"out/{tab}/se/{i}", lead.se)
+    _put(d, "efermi", np.array(0.1))
+    np.savez_compressed(os.path.join(HERE, "lead_property.npz"), **d)
+
+
 def _lopez_cases(sg_mod):
     d = {}
     chain = workload.chain_device(L=4)
@@ -476,7 +536,7 @@ def _adjoint_dos_case(rgf_mod, name, dims, B, seed, with_t, eta=1e-5):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default=ref_import.DEFAULT_REF_ROOT)
-    ap.add_argument("--only", default=None, help="regenerate one family: rgf, devprop, lopez, ozaki, adjoint, fiori, ozaki_integrate, current")
+    ap.add_argument("--only", default=None, help="regenerate one family: rgf, devprop, lopez, ozaki, adjoint, fiori, ozaki_integrate, current, lead_property")
     args = ap.parse_args()
     torch.set_num_threads(1)  # the container's threaded batched zgesv can hang
     rgf_mod = ref_import.load("recursive_green_cal", args.ref_root)
@@ -510,6 +570,8 @@ def main():
         _adjoint_dos_case(rgf_mod, "nonuniform", [6, 9, 5, 7], 3, seed=24, with_t=False)
         _adjoint_dos_case(rgf_mod, "uniform_with_t", [10] * 5, 2, seed=25, with_t=True)
         _adjoint_dos_case(rgf_mod, "single_block", [8], 2, seed=26, with_t=False)
+    if want("lead_property"):
+        _lead_property_case(ref_import.load("lead_property", args.ref_root))
     if want("current"):
         _current_case(dp_mod)
     if want("ozaki_integrate"):

@@ -430,3 +430,41 @@ def test_ozaki_integrate_matches_reference_fixture():
           f"DM_neq {_rel(DM_neq, g['out/DM_neq']):.2e}")
     assert _rel(DM_eq, g["out/DM_eq"]) < 1e-9
     assert _rel(DM_neq, g["out/DM_neq"]) < 1e-9
+
+
+class _LeadOnlyHamiltonian:
+    """Lead blocks shifted by the lead voltage (H - v S) and the device's sub-block sizes."""
+
+    def __init__(self, blocks, subblocks):
+        self.blocks, self.subblocks = blocks, subblocks
+
+    def get_hs_device(self, kpoint, V=None, block_tridiagonal=True, only_subblocks=False):
+        return self.subblocks
+
+    def get_hs_lead(self, kpoint, tab, v):
+        hL, hLL, hDL, sL, sLL, sDL = self.blocks[tab]
+        return hL - v * sL, hLL - v * sLL, hDL, sL, sLL, sDL
+
+
+def test_lead_property_self_energy_matches_reference_fixture():
+    """LeadProperty.self_energy against the reference's own: voltage-shifted lead layers, H_DL
+    trimmed to the coupled device block by HDL_reduced, E_ref = E_F, Python-float energies
+    (float32 as the reference's torch.tensor) and a complex tensor energy; each energy alone and
+    all three in one batched launch, within 1e-9 relative."""
+    from dpnegf_b200.lead_property import LeadProperty
+    g = Golden("lead_property")
+    blocks = {t: tuple(torch.as_tensor(g[f"{t}/{k}"]) for k in ("hL", "hLL", "hDL", "sL", "sLL", "sDL"))
+              for t in ("lead_L", "lead_R")}
+    ham = _LeadOnlyHamiltonian(blocks, [int(x) for x in g["subblocks"]])
+    energies = [-0.3, 0.25, torch.tensor(0.1 + 0.2j, dtype=torch.complex128)]
+    for tab in ("lead_L", "lead_R"):
+        lead = LeadProperty(tab, ham, None, "", voltage=float(g[f"{tab}/voltage"]), efermi=float(g["efermi"]))
+        want = [g[f"out/{tab}/se/{i}"] for i in range(3)]
+        for e, w in zip(energies, want):
+            lead.self_energy(kpoint=[0.0, 0.0, 0.0], energy=e, eta_lead=1e-5, save_path="/nonexistent-negf-se/x.h5")
+            assert tuple(lead.se.shape) == w.shape
+            assert _rel(lead.se, w) < 1e-9, (tab, e)
+        batch = torch.tensor([np.float32(-0.3), np.float32(0.25), 0.1 + 0.2j], dtype=torch.complex128)
+        lead.self_energy(kpoint=[0.0, 0.0, 0.0], energy=batch, eta_lead=1e-5)
+        for i, w in enumerate(want):
+            assert _rel(lead.se[i], w) < 1e-9, (tab, "batched", i)

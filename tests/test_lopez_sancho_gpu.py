@@ -99,3 +99,44 @@ def test_non_convergent_lead_reports_status():
     assert res.iters[0] <= 101
     with pytest.raises((RuntimeError, ArithmeticError)):
         self_energies(arena, [0], [0.3], 0.0)
+
+
+def test_lead_wider_coupling_than_layer():
+    """A coupled device block wider than the lead's principal layer (nc > n): the self-energy
+    products are nc x b and nc x nc, so the slot buffers are sized by max(n, nc); the result
+    matches the oracle for nc = 2n + 1."""
+    import torch
+    from dpnegf_b200.surface_green import LeadArena, LeadBlocks, self_energies
+    gen = torch.Generator().manual_seed(9)
+    c = lambda *s: torch.complex(torch.randn(*s, generator=gen, dtype=torch.float64),
+                                 torch.randn(*s, generator=gen, dtype=torch.float64))
+    n, nc = 6, 13
+    h = c(n, n) * 0.2
+    h = 0.5 * (h + h.mH) + torch.diag(torch.linspace(-1, 1, n, dtype=torch.float64)).to(torch.complex128)
+    s = torch.eye(n, dtype=torch.complex128)
+    hLL, sLL = 0.5 * c(n, n) / n ** 0.5, torch.zeros(n, n, dtype=torch.complex128)
+    hDL, sDL = 0.5 * c(nc, n) / n ** 0.5, 0.01 * c(nc, n) / n ** 0.5
+    arena = LeadArena([LeadBlocks(h, hLL, s, sLL, hDL, sDL)])
+    assert arena.max_n == nc
+    E = np.array([-0.4, 0.3 + 0.1j])
+    got = self_energies(arena, [0, 0], E, 1e-5)
+    for i, e in enumerate(E):
+        want = lead_oracle.self_energy(h.numpy(), hLL.numpy(), s.numpy(), sLL.numpy(), e, hDL.numpy(),
+                                       sDL.numpy(), etaLead=1e-5)[0]
+        assert got.sigma[i].shape == (nc, nc)
+        err = np.abs(got.sigma[i].cpu().numpy() - want).max() / np.abs(want).max()
+        assert err < 1e-9, err
+
+
+def test_item_with_lead_above_max_n_is_refused():
+    """A problem whose max_n is below a lead's size: every item gets NEGF_ERR_ARGUMENT from the
+    kernel (checked before any slot buffer is touched) and the host raises ValueError."""
+    import torch
+    from dpnegf_b200.surface_green import LeadArena, LeadBlocks, self_energies
+    n = 8
+    h = torch.diag(torch.linspace(-1, 1, n, dtype=torch.float64)).to(torch.complex128)
+    eye = torch.eye(n, dtype=torch.complex128)
+    arena = LeadArena([LeadBlocks(h, 0.5 * eye, eye, 0 * eye)])
+    arena.max_n = 4
+    with pytest.raises(ValueError, match="larger than the problem's max_n"):
+        self_energies(arena, [0, 0], [0.1, 0.2], 1e-5)

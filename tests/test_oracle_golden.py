@@ -192,3 +192,21 @@ def test_current_nscf_matches_reference():
     np.testing.assert_array_equal(v2.numpy(), g["out/vv"])
     c2 = np.array([float(c) for c in c2])
     assert np.abs(c2 - g["out/cc"]).max() < 1e-12 * np.abs(g["out/cc"]).max()
+
+
+def test_lead_self_energy_restatement_matches_reference_lead_property():
+    """The Lopez-Sancho + self-energy restatement against the reference's LeadProperty.self_energy
+    (voltage-shifted lead layers, H_DL trimmed to the coupled device block, E_ref = E_F,
+    Python-float energies rounded to float32 as the reference's torch.tensor does): 1e-9."""
+    g = Golden("lead_property")
+    sub = [int(x) for x in g["subblocks"]]
+    energies = [float(np.float32(-0.3)), float(np.float32(0.25)), 0.1 + 0.2j]
+    for tab in ("lead_L", "lead_R"):
+        hL, hLL, hDL, sL, sLL, sDL = (g[f"{tab}/{k}"] for k in ("hL", "hLL", "hDL", "sL", "sLL", "sDL"))
+        v = float(g[f"{tab}/voltage"])
+        rows = slice(0, sub[0]) if tab == "lead_L" else slice(hDL.shape[0] - sub[-1], hDL.shape[0])
+        for i, e in enumerate(energies):
+            se = lead_oracle.self_energy(hL - v * sL, hLL - v * sLL, sL, sLL, e, hDL[rows], sDL[rows],
+                                         etaLead=1e-5, E_ref=float(g["efermi"]))[0]
+            want = g[f"out/{tab}/se/{i}"]
+            assert np.abs(se - want).max() < 1e-9 * np.abs(want).max(), (tab, i)

@@ -365,6 +365,8 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
                 t = t.to(device=dev, dtype=C128)
                 if t.ndim == 2:
                     t = t.unsqueeze(0).expand(B, -1, -1)
+                if tuple(t.shape) != (B, dims[q], dims[q]):
+                    raise ValueError(f"s_in[{q}] has shape {tuple(t.shape)}, expected {(B, dims[q], dims[q])}")
                 blocks[b0 + q]["s_in"] = sin_cursor
                 sin_pieces.append(t.reshape(-1))
                 sin_cursor += B * dims[q] * dims[q]
@@ -376,6 +378,8 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
                 t = t.to(device=dev, dtype=C128)
                 if t.ndim == 2:
                     t = t.unsqueeze(0).expand(B, -1, -1)
+                if tuple(t.shape) != (B, dims[q], dims[q]):
+                    raise ValueError(f"s_out[{q}] has shape {tuple(t.shape)}, expected {(B, dims[q], dims[q])}")
                 blocks[b0 + q]["s_out"] = sout_cursor
                 sout_pieces.append(t.reshape(-1))
                 sout_cursor += B * dims[q] * dims[q]

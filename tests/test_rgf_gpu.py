@@ -265,3 +265,18 @@ def test_empty_energy_batch_gives_empty_blocks():
     geom = rgf_plan.Geometry([rgf_plan.DeviceBlocks(dev.hd, dev.hu, dev.hl, dev.sd, dev.su, dev.sl)])
     res = rgf_plan.run(geom, [E], [se], [se], eta=1e-5, outputs=(), trans=True, dos=True)
     assert res.trans.numel() == 0 and res.dos.numel() == 0
+
+
+def test_lesser_input_of_wrong_shape_is_refused():
+    """An s_in block whose shape is not [B, n_q, n_q] raises ValueError before any launch (a
+    wrong size would shift every later block of the packed lesser inputs)."""
+    from dpnegf_b200 import rgf_plan, workload
+    dims = [4, 5, 4]
+    dev = workload.random_device(0, 0, seed=2, block_dims=dims)
+    geom = rgf_plan.Geometry([rgf_plan.DeviceBlocks(dev.hd, dev.hu, dev.hl, dev.sd, dev.su, dev.sl)])
+    E = torch.linspace(-0.5, 0.5, 3, dtype=torch.float64).to(torch.complex128).cuda()
+    se = workload.random_self_energy(3, 4, seed=3).cuda()
+    s_in = [torch.zeros(3, n, n, dtype=torch.complex128, device="cuda") for n in dims]
+    s_in[1] = torch.zeros(3, 4, 4, dtype=torch.complex128, device="cuda")
+    with pytest.raises(ValueError, match=r"s_in\[1\] has shape"):
+        rgf_plan.run(geom, [E], [se], [se], eta=1e-5, outputs=("gnd",), s_in=[s_in])

@@ -129,7 +129,8 @@ typedef struct NegfRgfProblem {
   const NegfDevice* devices; /* device memory */
   const NegfItem* items;    /* device memory, processed in this order */
   int32_t n_items;
-  int32_t max_n;            /* largest n_q over all devices (<= NEGF_MAX_BLOCK) */
+  int32_t max_n;            /* largest n_q over all devices (<= NEGF_MAX_BLOCK); with max_g_slab and
+                               col_slab it sizes every slot, and the kernel trusts the tables to fit */
   int64_t max_g_slab;       /* largest g slab over all devices */
   const double* hs;         /* complex128 arena of H/S blocks */
   const double* s_in;       /* complex128 arena of Sigma^in blocks (NEGF_LESSER) */

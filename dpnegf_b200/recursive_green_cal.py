@@ -62,8 +62,8 @@ def recursive_gf(energy, hl, hd, hu, sd, su, sl, left_se, right_se, seP=None, E_
     B = int(shift.shape[0])
     K = len(hd)
 
-    if seP is not None:
-        hd = [h + p if torch.is_tensor(p) else h for h, p in zip(hd, seP)]
+    if seP is not None:  # added to the diagonal blocks as the reference does, numbers included (:411-414)
+        hd = [h if p is None else h + (p.to(h.device) if torch.is_tensor(p) else p) for h, p in zip(hd, seP)]
 
     per_energy = any(_is3(t) for lst in (hd, hu, hl, sd, su, sl) for t in lst)
     if per_energy:

@@ -9,7 +9,7 @@ seeded inputs together with the reference's own outputs:
 
   rgf_*.npz       ``recursive_gf`` (negf/recursive_green_cal.py:324) retarded,
                   lesser and greater cases, uniform and non-uniform blocks,
-                  batched and scalar energies;
+                  batched and scalar energies, per-block self-energies ``seP``;
   devprop_*.npz   ``DeviceProperty.cal_green_function`` + ``_cal_tc_`` /
                   ``_cal_dos_`` / ``_cal_ldos_`` (negf/device_property.py)
                   driven through the same fakes the reference tests use;
@@ -75,7 +75,7 @@ def _put(d, key, val):
 
 
 def _rgf_case(rgf_mod, name, dims, B, seed, lesser=False, greater=False, scalar=False,
-              gr_lc=True, eta=1e-5, E_ref=0.0):
+              gr_lc=True, eta=1e-5, E_ref=0.0, sep=False):
     dev = workload.random_device(0, 0, seed=seed, block_dims=dims)
     seL = workload.random_self_energy(B, dims[0], seed=seed + 100)
     seR = workload.random_self_energy(B, dims[-1], seed=seed + 200)
@@ -94,8 +94,13 @@ def _rgf_case(rgf_mod, name, dims, B, seed, lesser=False, greater=False, scalar=
             x = torch.complex(torch.randn(B, n, n, generator=gen, dtype=torch.float64),
                               torch.randn(B, n, n, generator=gen, dtype=torch.float64))
             s_out.append(0.5 * (x + x.mH))
+    seP = None
+    if sep:  # per-block self-energy: energy independent (2-D), a 0 placeholder, per energy (3-D)
+        c = lambda *sh: torch.complex(torch.randn(*sh, generator=gen, dtype=torch.float64),
+                                      -torch.rand(*sh, generator=gen, dtype=torch.float64)) * 0.05
+        seP = [c(n, n) if q % 3 == 0 else (0 if q % 3 == 1 else c(B, n, n)) for q, n in enumerate(dims)]
     kw = dict(hl=dev.hl, hd=dev.hd, hu=dev.hu, sd=dev.sd, su=dev.su, sl=dev.sl, eta=eta,
-              E_ref=E_ref, need_lesser=lesser, need_greater=greater, need_gr_lc=gr_lc)
+              E_ref=E_ref, need_lesser=lesser, need_greater=greater, need_gr_lc=gr_lc, seP=seP)
     if scalar:
         assert B == 1
         ans = rgf_mod.recursive_gf(E[0], left_se=seL[0], right_se=seR[0],
@@ -113,6 +118,8 @@ def _rgf_case(rgf_mod, name, dims, B, seed, lesser=False, greater=False, scalar=
         _put(d, k, getattr(dev, k))
     _put(d, "left_se", seL)
     _put(d, "right_se", seR)
+    if sep:
+        _put(d, "seP", seP)
     if lesser:
         _put(d, "s_in", s_in)
     if greater:
@@ -556,6 +563,7 @@ def main():
         _rgf_case(rgf_mod, "greater", [4, 5, 4], 3, seed=6, greater=True, lesser=True)
         _rgf_case(rgf_mod, "two_blocks", [3, 3], 2, seed=8)
         _rgf_case(rgf_mod, "wide_uniform", [20] * 4, 2, seed=9, gr_lc=False)
+        _rgf_case(rgf_mod, "scattering_seP", [6, 7, 5, 6], 3, seed=10, sep=True)
     if want("devprop"):
         _devprop_case(dp_mod, "nonuniform", [4, 5, 4], 5, seed=10, norbs=[2, 3, 1, 3, 4])
         _devprop_case(dp_mod, "uniform", [6] * 4, 4, seed=11, norbs=[1] * 24)

@@ -26,7 +26,8 @@ def run_oracle_on(g):
               need_lesser=g.has("s_in"), need_greater=g.has("s_out"),
               need_gr_lc=g.has("out/gr_lc"))
     return rgf_oracle.rgf(g["energy"], g["hl"], g["hd"], g["hu"], g["sd"], g["su"], g["sl"],
-                          g["left_se"], g["right_se"], s_in=g.get("s_in"), s_out=g.get("s_out"), **kw)
+                          g["left_se"], g["right_se"], seP=g.get("seP"), s_in=g.get("s_in"), s_out=g.get("s_out"),
+                          **kw)
 
 
 @pytest.mark.parametrize("case", rgf_cases())

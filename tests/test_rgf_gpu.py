@@ -49,6 +49,8 @@ def test_rgf_matches_reference_fixture(case):
     seL, seR = torch.as_tensor(g["left_se"]).cuda(), torch.as_tensor(g["right_se"]).cuda()
     lesser, greater = g.has("s_in"), g.has("s_out")
     kw = dict(eta=float(g["eta"]), E_ref=float(g["E_ref"]), need_gr_lc=g.has("out/gr_lc"))
+    if g.has("seP"):  # tensors per block, plain numbers (the reference's 0 placeholders) as numbers
+        kw["seP"] = [torch.as_tensor(x).cuda() if np.ndim(x) else complex(x) for x in g["seP"]]
     if scalar:
         ans = recursive_gf(E[0], _cu(g["hl"]), _cu(g["hd"]), _cu(g["hu"]), _cu(g["sd"]), _cu(g["su"]),
                            _cu(g["sl"]), seL[0], seR[0],

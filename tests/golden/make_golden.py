@@ -14,7 +14,8 @@ seeded inputs together with the reference's own outputs:
                   ``_cal_dos_`` / ``_cal_ldos_`` (negf/device_property.py)
                   driven through the same fakes the reference tests use;
   lopez_*.npz     ``surface_green`` / ``selfEnergy`` (negf/surface_green.py)
-                  for the 1-D chain lead and a random non-orthogonal lead;
+                  for the 1-D chain lead and a random non-orthogonal lead, and
+                  without H_DL (the bulk forms, ``Bulk`` off and on);
   ozaki.npz       ``ozaki_residues`` (negf/ozaki_res_cal.py) and ``gauss_xw``
                   (negf/negf_utils.py:136);
   adjoint_*.npz   gradients of sum_E w_E T(E) w.r.t. every H/S block and both
@@ -451,6 +452,29 @@ def _lopez_cases(sg_mod):
     np.savez_compressed(os.path.join(HERE, "lopez_sancho.npz"), **d)
 
 
+def _lopez_bulk_case(sg_mod):
+    """selfEnergy without H_DL: Sigma = (E S - H) - g_s^-1, and with Bulk=True g_s^-1 itself
+    (surface_green.py:73-80)."""
+    d = {}
+    ld = workload.random_device(6, 4, seed=8).lead_R
+    es = np.array([-1.3, 0.2, 0.9])
+    for bulk in (False, True):
+        sig_all, gs_all = [], []
+        for e in es:
+            sig, gs = sg_mod.selfEnergy(hL=ld.hL, hLL=ld.hLL, sL=ld.sL, sLL=ld.sLL, ee=float(e), etaLead=1e-5,
+                                        E_ref=0.05, Bulk=bulk)
+            sig_all.append(sig.numpy())
+            gs_all.append(gs.numpy())
+        _put(d, f"bulk{int(bulk)}/sigma", np.stack(sig_all))
+        _put(d, f"bulk{int(bulk)}/gs", np.stack(gs_all))
+    _put(d, "energy", es)
+    _put(d, "eta", np.array(1e-5))
+    _put(d, "E_ref", np.array(0.05))
+    for k in ("hL", "hLL", "sL", "sLL"):
+        _put(d, k, getattr(ld, k))
+    np.savez_compressed(os.path.join(HERE, "lopez_bulk.npz"), **d)
+
+
 def _ozaki_cases(oz_mod, nu_mod):
     d = {}
     for M in (30, 64):
@@ -543,7 +567,7 @@ def _adjoint_dos_case(rgf_mod, name, dims, B, seed, with_t, eta=1e-5):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default=ref_import.DEFAULT_REF_ROOT)
-    ap.add_argument("--only", default=None, help="regenerate one family: rgf, devprop, lopez, ozaki, adjoint, fiori, ozaki_integrate, current, lead_property")
+    ap.add_argument("--only", default=None, help="regenerate one family: rgf, devprop, lopez, ozaki, adjoint, fiori, ozaki_integrate, current, lead_property, lopez_bulk")
     args = ap.parse_args()
     torch.set_num_threads(1)  # the container's threaded batched zgesv can hang
     rgf_mod = ref_import.load("recursive_green_cal", args.ref_root)
@@ -569,6 +593,8 @@ def main():
         _devprop_case(dp_mod, "uniform", [6] * 4, 4, seed=11, norbs=[1] * 24)
     if want("lopez"):
         _lopez_cases(sg_mod)
+    if want("lopez_bulk"):
+        _lopez_bulk_case(sg_mod)
     if want("ozaki"):
         _ozaki_cases(oz_mod, nu_mod)
     if want("adjoint"):

@@ -140,3 +140,19 @@ def test_item_with_lead_above_max_n_is_refused():
     arena.max_n = 4
     with pytest.raises(ValueError, match="larger than the problem's max_n"):
         self_energies(arena, [0, 0], [0.1, 0.2], 1e-5)
+
+
+def test_self_energy_bulk_forms_match_reference_fixture():
+    """selfEnergy without H_DL on the GPU: (E S - H) - g_s^-1 and, with Bulk=True, g_s^-1 against
+    the reference's own selfEnergy, within 1e-9 relative."""
+    from dpnegf_b200.surface_green import selfEnergy
+    g = Golden("lopez_bulk")
+    blocks = {k: torch.as_tensor(g[k]) for k in ("hL", "hLL", "sL", "sLL")}
+    for bulk in (False, True):
+        for i, e in enumerate(g["energy"]):
+            sig, gs = selfEnergy(**blocks, ee=float(e), etaLead=float(g["eta"]), E_ref=float(g["E_ref"]), Bulk=bulk)
+            want = g[f"bulk{int(bulk)}/sigma"][i]
+            err = np.abs(sig.cpu().numpy() - want).max() / np.abs(want).max()
+            assert err < 1e-9, (bulk, i, err)
+            gerr = np.abs(gs.cpu().numpy() - g[f"bulk{int(bulk)}/gs"][i]).max() / np.abs(g[f"bulk{int(bulk)}/gs"][i]).max()
+            assert gerr < 1e-9, (bulk, i, gerr)

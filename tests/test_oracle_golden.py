@@ -211,3 +211,16 @@ def test_lead_self_energy_restatement_matches_reference_lead_property():
                                          etaLead=1e-5, E_ref=float(g["efermi"]))[0]
             want = g[f"out/{tab}/se/{i}"]
             assert np.abs(se - want).max() < 1e-9 * np.abs(want).max(), (tab, i)
+
+
+def test_self_energy_bulk_forms_match_reference():
+    """selfEnergy without H_DL: (E S - H) - g_s^-1 (and g_s^-1 with Bulk=True) against the
+    reference's own, 1e-9."""
+    g = Golden("lopez_bulk")
+    for i, e in enumerate(g["energy"]):
+        sig, gs, st, _ = lead_oracle.self_energy(g["hL"], g["hLL"], g["sL"], g["sLL"], e, etaLead=float(g["eta"]),
+                                                 E_ref=float(g["E_ref"]))
+        assert st in (lead_oracle.LS_OK, lead_oracle.LS_WARN)
+        _close(gs, g["bulk0/gs"][i], atol=1e-9, rtol=1e-8)
+        _close(sig, g["bulk0/sigma"][i], atol=1e-9, rtol=1e-8)
+        _close(np.linalg.inv(gs), g["bulk1/sigma"][i], atol=1e-9, rtol=1e-8)

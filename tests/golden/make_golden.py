@@ -155,7 +155,7 @@ class _FakeLead:
         return 1j * (self.se - self.se.mH)
 
 
-def _devprop_case(dp_mod, name, dims, B, seed, norbs, need_lesser=True):
+def _devprop_case(dp_mod, name, dims, B, seed, norbs, need_lesser=True, block_tridiagonal=True):
     dev = workload.random_device(0, 0, seed=seed, block_dims=dims)
     dev.norbs_per_atom = norbs
     seL = workload.random_self_energy(B, dims[0], seed=seed + 1)
@@ -180,7 +180,7 @@ def _devprop_case(dp_mod, name, dims, B, seed, norbs, need_lesser=True):
     dp.lead_L.se = seL
     dp.lead_R.se = seR
     dp.cal_green_function(energy=E, kpoint=[0.0, 0.0, 0.0], eta_device=1e-6,
-                          block_tridiagonal=True, need_lesser=need_lesser)
+                          block_tridiagonal=block_tridiagonal, need_lesser=need_lesser)
     d = {}
     _put(d, "dims", np.array(dims))
     _put(d, "norbs", np.array(norbs))
@@ -190,6 +190,7 @@ def _devprop_case(dp_mod, name, dims, B, seed, norbs, need_lesser=True):
     _put(d, "left_se", seL)
     _put(d, "right_se", seR)
     _put(d, "E_ref", np.array(0.05))
+    _put(d, "block_tridiagonal", np.array(block_tridiagonal))
     _put(d, "eta_device", np.array(1e-6))
     _put(d, "muL", np.array(0.1))
     _put(d, "muR", np.array(-0.1))
@@ -591,6 +592,7 @@ def main():
     if want("devprop"):
         _devprop_case(dp_mod, "nonuniform", [4, 5, 4], 5, seed=10, norbs=[2, 3, 1, 3, 4])
         _devprop_case(dp_mod, "uniform", [6] * 4, 4, seed=11, norbs=[1] * 24)
+        _devprop_case(dp_mod, "dense", [9], 4, seed=12, norbs=[2, 3, 4], block_tridiagonal=False)
     if want("lopez"):
         _lopez_cases(sg_mod)
     if want("lopez_bulk"):

@@ -62,14 +62,15 @@ def _devprop_from_golden(g):
     return dp
 
 
-@pytest.mark.parametrize("case", ["devprop_nonuniform", "devprop_uniform"])
+@pytest.mark.parametrize("case", ["devprop_nonuniform", "devprop_uniform", "devprop_dense"])
 def test_device_property_matches_reference_fixture(case):
     g = Golden(case)
     dp = _devprop_from_golden(g)
     dp.lead_L.se = torch.as_tensor(g["left_se"])
     dp.lead_R.se = torch.as_tensor(g["right_se"])
     dp.cal_green_function(energy=torch.as_tensor(g["energy"]), kpoint=[0.0, 0.0, 0.0],
-                          eta_device=float(g["eta_device"]), block_tridiagonal=True, need_lesser=True)
+                          eta_device=float(g["eta_device"]), block_tridiagonal=bool(g["block_tridiagonal"]),
+                          need_lesser=True)
     assert _rel(dp.tc, g["out/tc"]) < 1e-10
     assert _rel(dp.dos, g["out/dos"]) < 1e-10
     assert _rel(dp.ldos, g["out/ldos"]) < 1e-10

@@ -50,7 +50,7 @@ def test_rgf_oracle_matches_reference(case):
             _close(mine[0] if scalar else mine, ref)
 
 
-@pytest.mark.parametrize("case", ["devprop_nonuniform", "devprop_uniform"])
+@pytest.mark.parametrize("case", ["devprop_nonuniform", "devprop_uniform", "devprop_dense"])
 def test_device_traces_match_reference(case):
     g = Golden(case)
     E = g["energy"]

@@ -413,6 +413,26 @@ def _lead_property_case(lp_mod):
     np.savez_compressed(os.path.join(HERE, "lead_property.npz"), **d)
 
 
+def _onsite_case(dens_mod):
+    """Ozaki.get_density_onsite (negf/density.py:201-230): per-atom sums of diag(DM) beside the
+    atom positions, for a matrix and for a vector DM."""
+    from types import SimpleNamespace
+    gen = torch.Generator().manual_seed(51)
+    norbs = [2, 3, 1, 4]
+    n = sum(norbs)
+    DM = torch.randn(n, n, generator=gen, dtype=torch.float64)
+    pos = torch.randn(len(norbs), 3, generator=gen, dtype=torch.float64).numpy()
+    dp = SimpleNamespace(norbs_per_atom=norbs, structure=SimpleNamespace(positions=pos))
+    oz = dens_mod.Ozaki(R=1e6, M_cut=4, n_gauss=2)
+    d = {}
+    _put(d, "DM", DM)
+    _put(d, "norbs", np.array(norbs))
+    _put(d, "positions", pos)
+    _put(d, "out/matrix", oz.get_density_onsite(dp, DM))
+    _put(d, "out/vector", oz.get_density_onsite(dp, DM.diag() * 2))
+    np.savez_compressed(os.path.join(HERE, "density_onsite.npz"), **d)
+
+
 def _lopez_cases(sg_mod):
     d = {}
     chain = workload.chain_device(L=4)
@@ -568,7 +588,7 @@ def _adjoint_dos_case(rgf_mod, name, dims, B, seed, with_t, eta=1e-5):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default=ref_import.DEFAULT_REF_ROOT)
-    ap.add_argument("--only", default=None, help="regenerate one family: rgf, devprop, lopez, ozaki, adjoint, fiori, ozaki_integrate, current, lead_property, lopez_bulk")
+    ap.add_argument("--only", default=None, help="regenerate one family: rgf, devprop, lopez, ozaki, adjoint, fiori, ozaki_integrate, current, lead_property, lopez_bulk, onsite")
     args = ap.parse_args()
     torch.set_num_threads(1)  # the container's threaded batched zgesv can hang
     rgf_mod = ref_import.load("recursive_green_cal", args.ref_root)
@@ -608,6 +628,8 @@ def main():
         _adjoint_dos_case(rgf_mod, "single_block", [8], 2, seed=26, with_t=False)
     if want("lead_property"):
         _lead_property_case(ref_import.load("lead_property", args.ref_root))
+    if want("onsite"):
+        _onsite_case(dens_mod)
     if want("current"):
         _current_case(dp_mod)
     if want("ozaki_integrate"):

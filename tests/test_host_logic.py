@@ -53,3 +53,18 @@ def test_scf_loop_argument_checks():
                               device="cpu")
     with pytest.raises(ValueError, match="same orbitals"):
         ScfLoop(mixed, [None] * 2, [None] * 2, z, c, w, plan=object())
+
+
+def test_density_onsite_matches_reference():
+    """Ozaki.get_density_onsite (per-atom sums of diag(DM) beside the positions) against the
+    reference's own, for a matrix and a vector DM (plain torch, no GPU needed)."""
+    from types import SimpleNamespace
+    from dpnegf_b200.density import Ozaki
+    from tests.goldens import Golden
+    g = Golden("density_onsite")
+    dp = SimpleNamespace(norbs_per_atom=[int(x) for x in g["norbs"]],
+                         structure=SimpleNamespace(positions=g["positions"]))
+    oz = Ozaki(R=1e6, M_cut=4, n_gauss=2)
+    DM = torch.as_tensor(g["DM"])
+    np.testing.assert_array_equal(oz.get_density_onsite(dp, DM).numpy(), g["out/matrix"])
+    np.testing.assert_array_equal(oz.get_density_onsite(dp, DM.diag() * 2).numpy(), g["out/vector"])

@@ -28,6 +28,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -491,39 +493,93 @@ def traffic_per_point(b, L):
 
 
 def cpu_procs():
+    """(processes, rule): one single-thread process per core, capped by 1.5 GB of free memory per
+    process (each holds the b=256, L=64 device and its working blocks) and at 64."""
     n = os.cpu_count() or 1
+    rule = f"min(os.cpu_count()={n}"
     try:
         import psutil
         mem_gb = psutil.virtual_memory().available / 2 ** 30
         n = min(n, max(1, int(mem_gb // 1.5)))
+        rule += f", {mem_gb:.0f} GB available // 1.5 GB per process"
     except Exception:
         pass
-    return max(1, min(n, 64))
+    return max(1, min(n, 64)), rule + ", 64)"
 
 
-def cpu_baseline(args, seed, target_seconds=20.0):
-    """Oracle RGF on host cores over a bounded sample of the workload's energies."""
-    import numpy as np
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def workload_self_energies(B, b):
+    """The self-energies every step of the GPU arm uses (seeds 1 and 2), on the host."""
+    from dpnegf_b200 import workload
+    return workload.random_self_energy(B, b, seed=1), workload.random_self_energy(B, b, seed=2)
+
+
+def cpu_sample_indices(n_all, n_sample):
+    return np.unique(np.linspace(0, n_all - 1, n_sample).round().astype(np.int64))
+
+
+def cpu_baseline(args, seed, seL_h, seR_h, n_energies=0):
+    """Oracle RGF + T/DOS on the host cores over a bounded sample of one step's workload: the
+    device of k-seed ``seed`` at the sampled energies, with exactly the self-energies the GPU arm
+    uses there, so the sample doubles as a parity check of that step (``T``/``D``/``idx``)."""
     from oracle import cpu_baseline as cb
-    procs = cpu_procs()
-    nE = args.cpu_energies or 8 * procs  # about 10-20 s of host work
-    E = np.linspace(-3.0, 3.0, args.energies)[:: max(1, args.energies // nE)][:nE]
-    seL, seR = cb._self_energies(args.b, len(E), seed)
-    T, D, wall = cb.run_sample(args.b, args.L, seed, E, seL, seR, args.eta, procs)
-    return {"value": len(E) / wall, "unit": UNIT, "cores": procs, "kind": "port", "seconds": wall,
-            "energies": len(E),
-            "sample": f"{len(E)} energies of the b={args.b} L={args.L} workload (k-seed {seed}), "
-                      f"numpy oracle RGF + T/DOS, {procs} spawn processes x 1 BLAS thread, {wall:.1f} s"}
+    procs, rule = cpu_procs()
+    nE = n_energies or args.cpu_energies or 8 * procs  # about 10-20 s of host work
+    E_all = np.linspace(-3.0, 3.0, args.energies)
+    idx = cpu_sample_indices(args.energies, nE)
+    seL = seL_h[torch_index(idx)].numpy()
+    seR = seR_h[torch_index(idx)].numpy()
+    T, D, wall = cb.run_sample(args.b, args.L, seed, E_all[idx], seL, seR, args.eta, procs)
+    return {"value": len(idx) / wall, "unit": UNIT, "cores": procs, "kind": "port", "seconds": wall,
+            "energies": int(len(idx)), "cpu_model": cpu_model(), "cpu_count": os.cpu_count(),
+            "process_rule": rule,
+            "sample": f"{len(idx)} of the {args.energies} energies of the b={args.b} L={args.L} workload "
+                      f"(k-seed {seed}, the GPU arm's self-energies at those energies), numpy oracle RGF + "
+                      f"T/DOS, {procs} spawn processes x 1 BLAS thread, {wall:.1f} s",
+            "T": T, "D": D, "idx": idx}
+
+
+def torch_index(idx):
+    import torch
+    return torch.as_tensor(idx, dtype=torch.long)
+
+
+def public_baseline(base):
+    """The cpu_baseline object of the JSON line (without the sampled arrays)."""
+    return {k: v for k, v in base.items() if k not in ("T", "D", "idx")}
+
+
+def parity_vs_cpu(base, T_gpu, D_gpu):
+    """Max relative differences of the GPU arm's T(E) and DOS from the CPU oracle at the sampled
+    energies of the same device and self-energies."""
+    idx = base["idx"]
+    Tg, Dg = np.asarray(T_gpu)[idx], np.asarray(D_gpu)[idx]
+    rel = lambda g, c: float(np.max(np.abs(g - c) / np.maximum(np.abs(c), 1e-300)))
+    return {"t_max_rel_err": rel(Tg, base["T"]), "dos_max_rel_err": rel(Dg, base["D"]),
+            "t_max_abs_err": float(np.max(np.abs(Tg - base["T"]))), "energies": int(len(idx)),
+            "against": "oracle (numpy complex128 restatement of recursive_gf + _cal_tc_/_cal_dos_) on the "
+                       "same device, energies and self-energies"}
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    seL_h, seR_h = workload_self_energies(args.energies, args.b)
     vals, secs = [], []
     base = None
     for s in range(args.warmup + args.steps):
-        base = cpu_baseline(args, seed=1000 + s)
+        base = cpu_baseline(args, s, seL_h, seR_h)  # step s: the GPU arm's device of step s
         if s >= args.warmup:
             vals.append(base["value"])
             secs.append(base["seconds"])
@@ -536,7 +592,7 @@ def run_reference(args):
                                    f"eta={args.eta}, T(E)+DOS; each step a bounded sample of "
                                    f"{base['energies']} energies on the host cores",
                        "b": args.b, "L": args.L, "energies_per_step": base["energies"]},
-            "cpu_baseline": dict(base, value=v),
+            "cpu_baseline": dict(public_baseline(base), value=v),
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -547,12 +603,14 @@ def main():
     if args.impl == "reference":
         return run_reference(args)
 
-    # the CPU baseline pool is spawned before any CUDA work
-    cpu_line = None
+    # the CPU baseline pool is spawned before any CUDA work; it samples the first timed step
+    # (device k-seed = warm-up count) with the GPU arm's own self-energies
+    cpu_base = None
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    seL_h, seR_h = workload_self_energies(args.energies, args.b)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu_line = cpu_baseline(args, seed=0)
+        cpu_base = cpu_baseline(args, args.warmup, seL_h, seR_h)
 
     import torch
     import torch.distributed as dist
@@ -567,8 +625,6 @@ def main():
 
     b, L, B = args.b, args.L, args.energies
     E = torch.linspace(-3.0, 3.0, B, dtype=torch.float64).to(torch.complex128)
-    seL_h = workload.random_self_energy(B, b, seed=1)
-    seR_h = workload.random_self_energy(B, b, seed=2)
     seL, seR = seL_h.cuda(), seR_h.cuda()
     Ed = E.cuda()
     nsteps = args.warmup + args.steps
@@ -601,8 +657,11 @@ def main():
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record()
+    first = None
     for i in range(args.steps):
-        step(args.warmup + i, ev=kev[i])
+        r = step(args.warmup + i, ev=kev[i])
+        if first is None:  # first timed step: its T/DOS are checked against the CPU sample
+            first = r
     t1.record()
     torch.cuda.synchronize()
     barrier()
@@ -780,7 +839,9 @@ def main():
                            "b": b, "L": L, "energies_per_step": B, "k_per_step_per_gpu": 1,
                            "l2": "inputs larger than L2 (H/S arena 380 MiB per step, per-slot scratch 82 MiB x 148)",
                            "parallelism": f"k-realisations across {world} GPU(s)"},
-                "roofline": roof, "cpu_baseline": cpu_line, "e2e": e2e, "clocks": clk,
+                "roofline": roof, "cpu_baseline": public_baseline(cpu_base) if cpu_base else None,
+                "parity": parity_vs_cpu(cpu_base, first.trans.cpu().numpy(), first.dos.cpu().numpy())
+                if cpu_base else None, "e2e": e2e, "clocks": clk,
                 "gpu_launches": args.steps, "kernel_ms": kms}
         if phases:
             line["phases"] = phases

@@ -3,9 +3,7 @@
     python dpnegf_b200/csrc/build.py [--force]
 
 The library is the C ABI declared in include/negf_b200.h.  It is rebuilt when
-any source under csrc/ or the header is newer than the .so.  The same step
-builds ``dpnegf_b200/gemm_micro``, the standalone check-and-time driver of
-the two CTA GEMMs (csrc/gemm_micro.cu).
+any source under csrc/ or the header is newer than the .so.
 """
 import argparse
 import glob
@@ -18,7 +16,6 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 ROOT = os.path.dirname(PKG)
 OUT = os.path.join(PKG, "libnegf_b200.so")
-MICRO = os.path.join(PKG, "gemm_micro")
 SOURCES = ["rgf.cu", "rgf_noalloc.cu", "lopez_sancho.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-v"]
@@ -32,9 +29,9 @@ def _nvcc():
 
 
 def stale():
-    if not os.path.exists(OUT) or not os.path.exists(MICRO):
+    if not os.path.exists(OUT):
         return True
-    t = min(os.path.getmtime(OUT), os.path.getmtime(MICRO))
+    t = os.path.getmtime(OUT)
     deps = glob.glob(os.path.join(HERE, "*.cu")) + glob.glob(os.path.join(HERE, "*.cuh"))
     deps.append(os.path.join(ROOT, "include", "negf_b200.h"))
     return any(os.path.getmtime(d) > t for d in deps)
@@ -52,13 +49,6 @@ def build(force=False, verbose=False):
     if verbose:
         sys.stdout.write(r.stderr)
     os.replace(OUT + ".tmp", OUT)
-    flags = [f for f in NVCC_FLAGS if f not in ("-shared", "-fPIC", "-Xcompiler", "-Xptxas", "-v")]
-    cmd = [_nvcc()] + flags + ["-o", MICRO + ".tmp", os.path.join(HERE, "gemm_micro.cu")]
-    r = subprocess.run(cmd, capture_output=True, text=True)
-    if r.returncode != 0:
-        sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed (gemm_micro)")
-    os.replace(MICRO + ".tmp", MICRO)
     return OUT
 
 

@@ -129,9 +129,12 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
   bool converged = false;
   for (int iter = 1; iter <= P.max_iter + 1; ++iter) {
     it_n = iter;
-    // A = zS - eps
-    cta_shift_form(A, eps, S, z, cmk(-1.0, 0.0), (int)n2, smem);
-    bad |= cta_inverse<false>(A, n, n, Ainv, n, smem_raw, &pc, snap);
+    // Ainv = (zS - eps)^-1, right-stable: (zS - eps)^T is inverted by Gauss-Jordan (row
+    // operations, whose computed inverse Y has a small left residual Y A^T - I) and Y^T taken,
+    // so (zS - eps) Ainv - I is small as for the reference's LU solve
+    cta_transpose_shift(A, eps, S, z, cmk(-1.0, 0.0), n, n, smem);
+    bad |= cta_inverse<false>(A, n, n, T, n, smem_raw, &pc, snap);
+    cta_transpose_shift(Ainv, T, nullptr, cmk(0.0, 0.0), ONE, n, n, smem);
     gemm_ls<OP_N, OP_N>(smem, n, n, n, Ainv, n, alpha, n, Xa, n);
     gemm_ls<OP_N, OP_N>(smem, n, n, n, Ainv, n, beta, n, Xb, n);
     gemm_ls<OP_N, OP_N>(smem, n, n, n, beta, n, Xa, n, T, n);  // beta Xa
@@ -165,9 +168,10 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
     st = NEGF_ERR_LS_NOT_CONVERGED;
   } else {
     cplx* gs = it.gs ? reinterpret_cast<cplx*>(it.gs) : gsb;
-    // g_s = (zS - eps_s)^-1
-    cta_shift_form(A, epss, S, z, cmk(-1.0, 0.0), (int)n2, smem);
-    bad |= cta_inverse<false>(A, n, n, gs, n, smem_raw, &pc, snap);
+    // g_s = (zS - eps_s)^-1, right-stable as above: the residual below is a right residual
+    cta_transpose_shift(A, epss, S, z, cmk(-1.0, 0.0), n, n, smem);
+    bad |= cta_inverse<false>(A, n, n, T, n, smem_raw, &pc, snap);
+    cta_transpose_shift(gs, T, nullptr, cmk(0.0, 0.0), ONE, n, n, smem);
     // residual: (zS - H - (z s01 - h01) g_s (z s10 - h10)) g_s - I
     // z s01 - h01
 #pragma unroll 4

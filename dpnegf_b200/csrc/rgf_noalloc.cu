@@ -24,7 +24,12 @@
 //     ordering) race on it;
 //   * the first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (once per device, with that device current), so
-//     make that first call before any stream capture begins.
+//     make that first call before any stream capture begins;
+//   * that address is kept for the life of the process: after a
+//     cudaDeviceReset the module is loaded again and the array may move, so
+//     no call may follow a device reset;
+//   * negf_rgf_static_slots reports how many work slots a call will run, so a
+//     caller can see when the slot count was lowered to fit.
 #include <mutex>
 
 #include <cuda_runtime.h>
@@ -62,10 +67,8 @@ extern "C" {
 
 size_t negf_rgf_static_scratch_bytes(void) { return kStaticScratchBytes; }
 
-int negf_rgf_run_static(const NegfRgfProblem* p, void* stream) {
-  if (!p) return NEGF_ERR_ARGUMENT;
-  if (p->n_items <= 0) return NEGF_OK;
-  if (p->n_slots <= 0 || p->max_n <= 0) return NEGF_ERR_ARGUMENT;
+int negf_rgf_static_slots(const NegfRgfProblem* p) {
+  if (!p || p->n_slots <= 0 || p->max_n <= 0) return NEGF_ERR_ARGUMENT;
   if (p->max_n > NEGF_MAX_BLOCK) return NEGF_ERR_UNSUPPORTED;
   NegfRgfProblem q = *p;
   q.n_slots = 1;
@@ -75,7 +78,16 @@ int negf_rgf_run_static(const NegfRgfProblem* p, void* stream) {
   q.n_slots = 2;
   const size_t per_slot = negf_rgf_scratch_bytes(&q) - one;
   size_t fit = per_slot ? 1 + (kStaticScratchBytes - one) / per_slot : (size_t)p->n_slots;
-  q.n_slots = (int)(fit < (size_t)p->n_slots ? fit : (size_t)p->n_slots);
+  return (int)(fit < (size_t)p->n_slots ? fit : (size_t)p->n_slots);
+}
+
+int negf_rgf_run_static(const NegfRgfProblem* p, void* stream) {
+  if (!p) return NEGF_ERR_ARGUMENT;
+  if (p->n_items <= 0) return NEGF_OK;
+  const int slots = negf_rgf_static_slots(p);
+  if (slots <= 0) return slots;
+  NegfRgfProblem q = *p;
+  q.n_slots = slots;
   void* addr = nullptr;
   const int st = static_scratch_address(&addr);
   if (st != NEGF_OK) return st;

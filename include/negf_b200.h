@@ -247,6 +247,12 @@ int negf_rgf_run(const NegfRgfProblem* p, void* cuda_stream);
  * stream capture. */
 int negf_rgf_run_static(const NegfRgfProblem* p, void* cuda_stream);
 
+/* Work slots negf_rgf_run_static will run for this problem: p->n_slots lowered to what fits in
+ * the static array (>= 1), or NEGF_ERR_SCRATCH_LIMIT / NEGF_ERR_ARGUMENT / NEGF_ERR_UNSUPPORTED.
+ * Host-only arithmetic, no device access.  The array's address is looked up once per device and
+ * kept for the life of the process, so no negf_rgf_run_static call may follow a cudaDeviceReset. */
+int negf_rgf_static_slots(const NegfRgfProblem* p);
+
 /* Size in bytes of the static scratch array used by negf_rgf_run_static. */
 size_t negf_rgf_static_scratch_bytes(void);
 

@@ -21,7 +21,8 @@ import sys
 import types
 from unittest import mock
 
-DEFAULT_REF_ROOT = os.environ.get("DPNEGF_REF_ROOT", "/root/reference")
+# Where the reference source tree lies: no default; pass it, or set DPNEGF_REF_ROOT.
+ENV_REF_ROOT = "DPNEGF_REF_ROOT"
 _STUBBED = ("ase", "xitorch", "matplotlib", "h5py", "dptb", "pyinstrument")
 
 
@@ -54,8 +55,15 @@ class _StubFinder(importlib.abc.MetaPathFinder):
         return None
 
 
-def install(ref_root: str = DEFAULT_REF_ROOT):
-    """Make ``import dpnegf.negf.<module>`` resolve to the reference sources."""
+def ref_root_from_env():
+    """The reference source root named by ``DPNEGF_REF_ROOT``, or None."""
+    return os.environ.get(ENV_REF_ROOT) or None
+
+
+def install(ref_root: str):
+    """Make ``import dpnegf.negf.<module>`` resolve to the reference sources at ``ref_root``."""
+    if not ref_root:
+        raise ValueError(f"the reference source root is required (argument, or {ENV_REF_ROOT})")
     pkg_root = os.path.join(ref_root, "dpnegf")
     if not os.path.isdir(pkg_root):
         raise FileNotFoundError(f"reference source tree not found at {pkg_root}")
@@ -70,7 +78,7 @@ def install(ref_root: str = DEFAULT_REF_ROOT):
     return True
 
 
-def load(module: str, ref_root: str = DEFAULT_REF_ROOT):
+def load(module: str, ref_root: str):
     """``load("recursive_green_cal")`` -> the reference module object."""
     install(ref_root)
     return importlib.import_module(f"dpnegf.negf.{module}")

@@ -2,7 +2,7 @@
 
 Run from the repository root in a container that has the dpnegf sources:
 
-    python tests/golden/make_golden.py [--ref-root PATH]
+    python tests/golden/make_golden.py --ref-root PATH   (or DPNEGF_REF_ROOT=PATH)
 
 It imports the reference hot path through ``oracle/ref_import.py`` and records
 seeded inputs together with the reference's own outputs:
@@ -585,10 +585,43 @@ def _adjoint_dos_case(rgf_mod, name, dims, B, seed, with_t, eta=1e-5):
     np.savez_compressed(os.path.join(HERE, f"adjoint_dos_{name}.npz"), **d)
 
 
+def _hdf5_case(lp_mod):
+    """The self-energy cache format: the reference's ``write_to_hdf5`` (negf/lead_property.py:932-941)
+    for every (k, E) of a k grid and an energy grid, through the dict-backed h5py stand-in of
+    tests/fake_h5py.py; records the group / dataset names it creates and the data, and checks that
+    its ``read_from_hdf5`` (:944-951) returns them."""
+    from tests import fake_h5py
+    lp_mod.h5py = fake_h5py.module()
+    fake_h5py.FILES.clear()
+    kgrid = np.array([[0.0, 0.0, 0.0], [0.5, 0.0, 0.0], [0.25, -0.25, 0.125]])
+    egrid = np.array([-1.25, -0.1, 0.0, 0.123456789, 2.5])
+    gen = torch.Generator().manual_seed(61)
+    d = {}
+    _put(d, "kgrid", kgrid)
+    _put(d, "egrid", egrid)
+    names = []
+    for tab in ("L", "R"):
+        path = f"/fake/self_energy_lead{tab}.h5"
+        for ik, k in enumerate(kgrid):
+            for ie, e in enumerate(egrid):
+                se = torch.complex(torch.randn(3, 3, generator=gen, dtype=torch.float64),
+                                   torch.randn(3, 3, generator=gen, dtype=torch.float64))
+                lp_mod.write_to_hdf5(path, k, e, se)
+                _put(d, f"se/{tab}/{ik}/{ie}", se)
+                back = lp_mod.read_from_hdf5(path, k, e)
+                assert np.array_equal(back, se.numpy())
+        for g, dsets in fake_h5py.keys(path).items():
+            for ds in dsets:
+                names.append(f"{tab}|{g}|{ds}")
+    d["names"] = np.array(sorted(names))
+    np.savez_compressed(os.path.join(HERE, "hdf5_keys.npz"), **d)
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-root", default=ref_import.DEFAULT_REF_ROOT)
-    ap.add_argument("--only", default=None, help="regenerate one family: rgf, devprop, lopez, ozaki, adjoint, fiori, ozaki_integrate, current, lead_property, lopez_bulk, onsite")
+    ap.add_argument("--ref-root", default=ref_import.ref_root_from_env(), required=ref_import.ref_root_from_env() is None,
+                    help="root of the reference source tree (default: $DPNEGF_REF_ROOT)")
+    ap.add_argument("--only", default=None, help="regenerate one family: rgf, devprop, lopez, ozaki, adjoint, fiori, ozaki_integrate, current, lead_property, lopez_bulk, onsite, hdf5")
     args = ap.parse_args()
     torch.set_num_threads(1)  # the container's threaded batched zgesv can hang
     rgf_mod = ref_import.load("recursive_green_cal", args.ref_root)
@@ -628,6 +661,8 @@ def main():
         _adjoint_dos_case(rgf_mod, "single_block", [8], 2, seed=26, with_t=False)
     if want("lead_property"):
         _lead_property_case(ref_import.load("lead_property", args.ref_root))
+    if want("hdf5"):
+        _hdf5_case(ref_import.load("lead_property", args.ref_root))
     if want("onsite"):
         _onsite_case(dens_mod)
     if want("current"):

@@ -44,3 +44,50 @@ def test_static_scratch_rejects_oversized_problem():
     assert noalloc.static_scratch_bytes() == 64 << 20
     T, D, st, code = noalloc.transmission_dos_static(geom, E, seL, seR, eta=1e-5)
     assert code == noalloc.NEGF_ERR_SCRATCH_LIMIT
+
+
+def test_static_scratch_on_a_side_stream():
+    """The call waits for the stream it launched on, so results are complete on return."""
+    from dpnegf_b200 import noalloc, rgf_plan
+    geom, E, seL, seR = _case(b=48, L=5, B=40, seed=17)
+    ref = rgf_plan.run(geom, [E.cuda()], [seL], [seR], eta=1e-5, outputs=(), trans=True, dos=True)
+    T_ref, D_ref = ref.trans.cpu().numpy(), ref.dos.cpu().numpy()
+    side = torch.cuda.Stream()
+    for _ in range(2):
+        T, D, st, code = noalloc.transmission_dos_static(geom, E, seL, seR, eta=1e-5, stream=side)
+        assert code == 0
+        assert int((st != 0).sum()) == 0
+        np.testing.assert_allclose(T.cpu().numpy(), T_ref, rtol=RTOL, atol=1e-12)
+        np.testing.assert_allclose(D.cpu().numpy(), D_ref, rtol=RTOL, atol=1e-12)
+
+
+def test_static_scratch_lesser_and_orbital_outputs():
+    """A deferred plan with block outputs, the lesser sweep and per-orbital DOS, run once on its
+    own scratch and twice on the static array: the same numbers each time."""
+    from dpnegf_b200 import noalloc, rgf_plan
+    from oracle import rgf_oracle
+    b, L, B = 40, 4, 6
+    geom, E, seL, seR = _case(b=b, L=L, B=B, seed=23)
+    f = np.linspace(0.2, 0.8, B)
+    s_in = rgf_oracle.s_in_from_se(seL.cpu().numpy(), seR.cpu().numpy(), f, 1 - f, [b] * L)
+    s_in = [[torch.as_tensor(s).cuda() for s in s_in]]
+    kw = dict(eta=1e-5, outputs=("grd", "gnd"), trans=True, orb_dos=True, s_in=s_in, check=False, defer=True)
+    plan = rgf_plan.run(geom, [E.cuda()], [seL], [seR], **kw)
+    assert noalloc.static_slots(plan.prob) >= 1
+    plan.launch()
+    torch.cuda.synchronize()
+    ref = plan.result
+    want = {"trans": ref.trans.cpu().numpy(), "orb": ref.orb_dos.cpu().numpy(),
+            "grd": [x.cpu().numpy() for x in ref.blocks[0]["grd"]],
+            "gnd": [x.cpu().numpy() for x in ref.blocks[0]["gnd"]]}
+    for _ in range(2):
+        plan2 = rgf_plan.run(geom, [E.cuda()], [seL], [seR], **kw)
+        res, code = noalloc.run_plan_static(plan2)
+        assert code == 0
+        assert int((res.status.cpu() != 0).sum()) == 0
+        np.testing.assert_allclose(res.trans.cpu().numpy(), want["trans"], rtol=RTOL, atol=1e-12)
+        np.testing.assert_allclose(res.orb_dos.cpu().numpy(), want["orb"], rtol=RTOL, atol=1e-12)
+        for tag in ("grd", "gnd"):
+            for g, w in zip(res.blocks[0][tag], want[tag]):
+                scale = np.abs(w).max()
+                assert np.abs(g.cpu().numpy() - w).max() <= RTOL * scale, tag

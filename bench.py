@@ -58,6 +58,8 @@ def parse():
                          "'leads' (its lead decimation alone, --lead-devices devices) and 'scf' (b=512 SCF "
                          "loop captured as a CUDA graph); not in the default run")
     ap.add_argument("--lead-devices", type=int, default=128, help="devices whose leads the 'leads' leg decimates")
+    ap.add_argument("--lead-eta", type=float, default=1e-5, help="lead broadening of the 'leads' leg")
+    ap.add_argument("--no-leads", action="store_true", help="skip the metric device's lead decimation object")
     ap.add_argument("--uneven-devices", type=int, default=128, help="devices of the 'uneven' leg")
     ap.add_argument("--uneven-precisions", default="fp64,mixed,mixed_refined",
                     help="runs of the 'uneven' leg besides FP64: mixed, mixed_refined")
@@ -358,26 +360,55 @@ def _uneven_inputs(torch, n_devices, seed):
     return dict(devs=devs, leads=leads, work=work, kBT=kBT, mu_L=mu_L, vL=vL, vR=vR, oz=oz, fL=fL, fR=fR, z=z)
 
 
-def leads_leg(torch, peak, n_devices=128, seed=2024):
+def leads_leg(torch, peak, n_devices=128, seed=2024, eta=ETA_LEAD_SYNTH):
     """The uneven batch's decimation phase alone: both leads of every device at every energy in one
     Lopez-Sancho launch, timed with CUDA events, with its algorithmic FP64 rate against the
     measured DGEMM peak (per-item doubling steps from the kernel's own iteration counts)."""
-    import numpy as np
     from dpnegf_b200.surface_green import LeadArena, self_energies
     u = _uneven_inputs(torch, n_devices, seed)
     nE = len(u["z"])
     arena = LeadArena([ld for pair in u["leads"] for ld in pair])
     idx = np.repeat(np.arange(2 * n_devices), nE)
-    self_energies(arena, idx[:2 * nE], np.tile(u["z"], 2), ETA_LEAD_SYNTH)  # warm-up: module load, first launch
-    res, ms = _timed(torch, lambda: self_energies(arena, idx, np.tile(u["z"], 2 * n_devices), ETA_LEAD_SYNTH))
+    self_energies(arena, idx[:2 * nE], np.tile(u["z"], 2), eta, check=False)  # warm-up: module load
+    res, ms = _timed(torch, lambda: self_energies(arena, idx, np.tile(u["z"], 2 * n_devices), eta, check=False))
     n = np.array([arena.shapes[i][0] for i in idx], dtype=np.float64)
     flops = float(_ls_flops(n, res.iters.astype(np.float64)).sum())
     ach = flops / (ms * 1e-3) / 1e12
-    return {"items": int(len(idx)), "n": "16..256", "seconds": ms * 1e-3, "value": len(idx) / (ms * 1e-3),
-            "unit": "decimations/s", "mean_iters": float(res.iters.mean()), "max_iters": int(res.iters.max()),
+    return {"items": int(len(idx)), "n": "16..256", "eta": eta, "seconds": ms * 1e-3,
+            "value": len(idx) / (ms * 1e-3), "unit": "decimations/s", "mean_iters": float(res.iters.mean()),
+            "max_iters": int(res.iters.max()), "status_counts": _status_counts(res.status),
             "roofline": {"achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
-                         "algorithmic": "8 (7/3 + 4) n^3 per doubling step x steps + 16 n^3 per item"},
-            "note": ETA_LEAD_NOTE}
+                         "algorithmic": "8 (7/3 + 4) n^3 per doubling step x steps + 16 n^3 per item"}}
+
+
+def _status_counts(st):
+    names = {0: "ok", 1: "warn_residual_1e-8", 2: "not_converged", 3: "residual_above_3e-5", 4: "singular"}
+    v, c = np.unique(np.asarray(st), return_counts=True)
+    return {names.get(int(a), str(int(a))): int(b) for a, b in zip(v, c)}
+
+
+def metric_leads_leg(torch, peak, dev, E, eta=1e-5, n_energies=512):
+    """Both leads of the metric device (its first / last block pairs repeated, b = 256) at
+    ``n_energies`` energies of the grid, eta = 1e-5, one decimation launch: decimations/s, mean
+    doubling steps and the algorithmic FP64 rate against the measured DGEMM peak."""
+    from dpnegf_b200.surface_green import LeadArena, LeadBlocks, self_energies
+    lb = lambda ld: LeadBlocks(ld.hL, ld.hLL, ld.sL, ld.sLL, ld.hDL, ld.sDL)
+    arena = LeadArena([lb(dev.lead_L), lb(dev.lead_R)])
+    Es = np.asarray(E.real.cpu().numpy())[cpu_sample_indices(len(E), n_energies)]
+    idx = np.repeat([0, 1], len(Es))
+    zz = np.tile(Es, 2)
+    self_energies(arena, idx[:64], zz[:64], eta, check=False)  # warm-up
+    res, ms = _timed(torch, lambda: self_energies(arena, idx, zz, eta, check=False))
+    n = float(arena.shapes[0][0])
+    flops = float(_ls_flops(n, res.iters.astype(np.float64)).sum())
+    ach = flops / (ms * 1e-3) / 1e12
+    return {"value": len(idx) / (ms * 1e-3), "unit": "decimations/s", "n": int(n), "items": int(len(idx)),
+            "eta": eta, "iters_mean": float(res.iters.mean()), "seconds": ms * 1e-3,
+            "status_counts": _status_counts(res.status),
+            "roofline": {"achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+                         "algorithmic": "8 (7/3 + 4) n^3 per doubling step x steps + 16 n^3 per item "
+                                        "(LU solve with 2n right-hand sides + 4 products per step)"},
+            "workload": f"both edge-pair leads of the b=256 metric device, {len(Es)} energies of [-3, 3] eV"}
 
 
 def uneven_leg(torch, n_devices=128, seed=2024, precisions=("fp64", "mixed", "mixed_refined")):
@@ -764,6 +795,11 @@ def main():
                            "adjoint launch time / T-only forward time; 1 warm-up + 1 timed step each")
 
     # the reference's own GPU path (torch complex128 solve + matmul) on a sample of the same workload
+    # lead self-energies of the metric device at eta = 1e-5 (rank 0)
+    leads = None
+    if rank == 0 and not args.no_leads and devs[args.warmup].lead_L is not None:
+        leads = metric_leads_leg(torch, peak, devs[args.warmup], E)
+
     torch_ref = None
     if rank == 0 and args.torch_energies > 0:
         d = devs[args.warmup]
@@ -792,7 +828,7 @@ def main():
     if rank == 0 and args.configs:
         wanted = [x.strip() for x in args.configs.split(",") if x.strip()]
         if "leads" in wanted:
-            extra["config3_leads"] = leads_leg(torch, peak, n_devices=args.lead_devices)
+            extra["config3_leads"] = leads_leg(torch, peak, n_devices=args.lead_devices, eta=args.lead_eta)
         if "uneven" in wanted:
             extra["config3_uneven"] = uneven_leg(torch, n_devices=args.uneven_devices,
                                                  precisions=args.uneven_precisions.split(","))
@@ -850,6 +886,8 @@ def main():
             line["adjoint"] = adjoint
         if torch_ref:
             line["torch_gpu_reference"] = torch_ref
+        if leads:
+            line["leads"] = leads
         line.update(extra)
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -8,7 +8,8 @@
 // (negf/surface_green.py:102-159) step for step:
 //   alpha = h10 - z s10,  beta = h01 - z s01,  eps = eps_s = H
 //   repeat (at most max_iter + 1 times):
-//     Xa = (zS - eps)^-1 alpha,  Xb = (zS - eps)^-1 beta
+//     [Xa Xb] = (zS - eps)^-1 [alpha beta]      (one LU solve, as the reference's
+//                                                np.linalg.solve with stacked right-hand sides)
 //     eps += alpha Xb + beta Xa;  eps_s += beta Xa
 //     alpha <- alpha Xa;  beta <- beta Xb
 //     stop when max(|alpha| + |beta|) < tol
@@ -23,7 +24,7 @@
 // or the bulk form Sigma = (E S - H) - g_s^-1 when the lead has no H_DL.
 #include <cstdio>
 #include "../../include/negf_b200.h"
-#include "cta_inverse.cuh"
+#include "cta_lu.cuh"
 #include "cta_stream.cuh"
 
 namespace negf {
@@ -33,7 +34,7 @@ constexpr size_t LS_SCRATCH_HEADER = 256;
 
 __host__ __device__ inline size_t ls_slot_elems(const NegfLsProblem& p) {
   size_t mn2 = (size_t)p.max_n * p.max_n;
-  size_t e = LS_NBUF * mn2 + inv_snapshot_elems(p.max_n);
+  size_t e = LS_NBUF * mn2;
   return (e + 15) & ~(size_t)15;
 }
 
@@ -109,15 +110,20 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
   const cplx E = cmk(it.e_re, it.e_im);
   const cplx z = cmk(it.e_re, it.e_im + it.eta);
   const cplx ONE = cmk(1.0, 0.0);
-  PhaseClock pc;
-  pc.start(false);
   cplx* b_[LS_NBUF];
   for (int i = 0; i < LS_NBUF; ++i) b_[i] = slot + i * mn2;
   cplx *eps = b_[0], *epss = b_[1], *alpha = b_[2], *beta = b_[3], *alpha2 = b_[4], *beta2 = b_[5];
-  cplx *A = b_[6], *Ainv = b_[7], *Xa = b_[8], *Xb = b_[9], *T = b_[10], *gsb = b_[11], *t1 = b_[12],
-       *t2 = b_[13];
-  cplx* snap = slot + LS_NBUF * mn2;
+  // Xab = [Xa Xb] (n x 2n, row stride 2n) spans b_[8] and b_[9]; b_[7] is spare
+  cplx *A = b_[6], *Xab = b_[8], *T = b_[10], *gsb = b_[11], *t1 = b_[12], *t2 = b_[13];
+  cplx *Xa = Xab, *Xb = Xab + n;
+  cplx *Ya = b_[8], *Yb = b_[9];  // separate n x n work blocks once the doubling is done
+  const int n2c = 2 * n;
   int bad = 0;
+  // out = I (n x n)
+  auto set_eye = [&](cplx* out) {
+    for (int e = threadIdx.x; e < n2; e += CTA_THREADS) out[e] = cmk(e / n == e % n ? 1.0 : 0.0, 0.0);
+    __syncthreads();
+  };
 
   // alpha = h10 - z s10 = h01^H - z s01^H ; beta = h01 - z s01 ; eps = eps_s = H
   form_herm_shift(alpha, h01, s01, z, n);
@@ -129,15 +135,16 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
   bool converged = false;
   for (int iter = 1; iter <= P.max_iter + 1; ++iter) {
     it_n = iter;
-    // Ainv = (zS - eps)^-1, right-stable: (zS - eps)^T is inverted by Gauss-Jordan (row
-    // operations, whose computed inverse Y has a small left residual Y A^T - I) and Y^T taken,
-    // so (zS - eps) Ainv - I is small as for the reference's LU solve
-    cta_transpose_shift(A, eps, S, z, cmk(-1.0, 0.0), n, n, smem);
-    bad |= cta_inverse<false>(A, n, n, T, n, smem_raw, &pc, snap);
-    cta_transpose_shift(Ainv, T, nullptr, cmk(0.0, 0.0), ONE, n, n, smem);
-    gemm_ls<OP_N, OP_N>(smem, n, n, n, Ainv, n, alpha, n, Xa, n);
-    gemm_ls<OP_N, OP_N>(smem, n, n, n, Ainv, n, beta, n, Xb, n);
-    gemm_ls<OP_N, OP_N>(smem, n, n, n, beta, n, Xa, n, T, n);  // beta Xa
+    // A = zS - eps;  [Xa Xb] = A^-1 [alpha beta]
+    cta_shift_form(A, eps, S, z, cmk(-1.0, 0.0), (int)n2, smem);
+    for (int e = threadIdx.x; e < n2; e += CTA_THREADS) {
+      const int i = e / n, j = e % n;
+      Xab[(int64_t)i * n2c + j] = alpha[e];
+      Xab[(int64_t)i * n2c + n + j] = beta[e];
+    }
+    __syncthreads();
+    bad |= cta_lu_solve(A, n, n, Xab, n2c, n2c, smem_raw);
+    gemm_ls<OP_N, OP_N>(smem, n, n, n, beta, n, Xa, n2c, T, n);  // beta Xa
     // eps_s += beta Xa ; eps += beta Xa (then + alpha Xb below)
 #pragma unroll 4
     for (int e = threadIdx.x; e < n2; e += CTA_THREADS) {
@@ -145,9 +152,9 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
       eps[e] = cadd(eps[e], T[e]);
     }
     __syncthreads();
-    gemm_ls<OP_N, OP_N>(smem, n, n, n, alpha, n, Xb, n, eps, n, eps, n);  // eps += alpha Xb
-    gemm_ls<OP_N, OP_N>(smem, n, n, n, alpha, n, Xa, n, alpha2, n);        // alpha <- alpha Xa
-    gemm_ls<OP_N, OP_N>(smem, n, n, n, beta, n, Xb, n, beta2, n);          // beta <- beta Xb
+    gemm_ls<OP_N, OP_N>(smem, n, n, n, alpha, n, Xb, n2c, eps, n, eps, n);  // eps += alpha Xb
+    gemm_ls<OP_N, OP_N>(smem, n, n, n, alpha, n, Xa, n2c, alpha2, n);        // alpha <- alpha Xa
+    gemm_ls<OP_N, OP_N>(smem, n, n, n, beta, n, Xb, n2c, beta2, n);          // beta <- beta Xb
     cplx* t = alpha; alpha = alpha2; alpha2 = t;
     t = beta; beta = beta2; beta2 = t;
     double m = 0.0;
@@ -168,10 +175,10 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
     st = NEGF_ERR_LS_NOT_CONVERGED;
   } else {
     cplx* gs = it.gs ? reinterpret_cast<cplx*>(it.gs) : gsb;
-    // g_s = (zS - eps_s)^-1, right-stable as above: the residual below is a right residual
-    cta_transpose_shift(A, epss, S, z, cmk(-1.0, 0.0), n, n, smem);
-    bad |= cta_inverse<false>(A, n, n, T, n, smem_raw, &pc, snap);
-    cta_transpose_shift(gs, T, nullptr, cmk(0.0, 0.0), ONE, n, n, smem);
+    // g_s = (zS - eps_s)^-1 by the LU solve against I (numpy.linalg.inv's route)
+    cta_shift_form(A, epss, S, z, cmk(-1.0, 0.0), (int)n2, smem);
+    set_eye(gs);
+    bad |= cta_lu_solve(A, n, n, gs, n, n, smem_raw);
     // residual: (zS - H - (z s01 - h01) g_s (z s10 - h10)) g_s - I
     // z s01 - h01
 #pragma unroll 4
@@ -179,16 +186,16 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
     __syncthreads();
     // z s10 - h10 = z s01^H - h01^H
     form_eS_minus_h_herm(t2, h01, s01, z, n, n);
-    gemm_ls<OP_N, OP_N>(smem, n, n, n, t1, n, gs, n, Xa, n);  // (z s01 - h01) g_s
-    gemm_ls<OP_N, OP_N>(smem, n, n, n, Xa, n, t2, n, Xb, n);  // ... (z s10 - h10)
-    // test = zS - H - Xb
+    gemm_ls<OP_N, OP_N>(smem, n, n, n, t1, n, gs, n, Ya, n);  // (z s01 - h01) g_s
+    gemm_ls<OP_N, OP_N>(smem, n, n, n, Ya, n, t2, n, Yb, n);  // ... (z s10 - h10)
+    // test = zS - H - Yb
 #pragma unroll 4
-    for (int e = threadIdx.x; e < n2; e += CTA_THREADS) T[e] = csub(csub(cmul(z, S[e]), H[e]), Xb[e]);
+    for (int e = threadIdx.x; e < n2; e += CTA_THREADS) T[e] = csub(csub(cmul(z, S[e]), H[e]), Yb[e]);
     __syncthreads();
-    gemm_ls<OP_N, OP_N>(smem, n, n, n, T, n, gs, n, Xa, n);  // test g_s
+    gemm_ls<OP_N, OP_N>(smem, n, n, n, T, n, gs, n, Ya, n);  // test g_s
     double m = 0.0;
     for (int e = threadIdx.x; e < n2; e += CTA_THREADS) {
-      cplx v = Xa[e];
+      cplx v = Ya[e];
       if (e / n == e % n) v.x -= 1.0;
       double a = hypot(v.x, v.y);
       m = (a == a) ? fmax(m, a) : INFINITY;
@@ -208,14 +215,15 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
         __syncthreads();
         // t2 = E S_DL^H - H_DL^H (b x nc)
         form_eS_minus_h_herm(t2, hdl, sdl, E, b, nc);
-        gemm_ls<OP_N, OP_N>(smem, nc, b, b, t1, b, gs, n, Xa, b);   // (E S_DL - H_DL) g_s[:b,:b]
-        gemm_ls<OP_N, OP_N>(smem, nc, nc, b, Xa, b, t2, nc, sig, nc);
+        gemm_ls<OP_N, OP_N>(smem, nc, b, b, t1, b, gs, n, Ya, b);   // (E S_DL - H_DL) g_s[:b,:b]
+        gemm_ls<OP_N, OP_N>(smem, nc, nc, b, Ya, b, t2, nc, sig, nc);
       } else {
         // bulk form: Sigma = (E S - H) - g_s^-1
         cta_shift_form(A, gs, nullptr, cmk(0.0, 0.0), ONE, (int)n2, smem);
-        bad |= cta_inverse<false>(A, n, n, Xa, n, smem_raw, &pc, snap);
+        set_eye(Ya);
+        bad |= cta_lu_solve(A, n, n, Ya, n, n, smem_raw);
 #pragma unroll 4
-        for (int e = threadIdx.x; e < n2; e += CTA_THREADS) sig[e] = csub(csub(cmul(E, S[e]), H[e]), Xa[e]);
+        for (int e = threadIdx.x; e < n2; e += CTA_THREADS) sig[e] = csub(csub(cmul(E, S[e]), H[e]), Ya[e]);
         __syncthreads();
       }
     }
@@ -248,7 +256,7 @@ __global__ void __launch_bounds__(CTA_THREADS, 1) ls_kernel(const NegfLsProblem 
 }
 
 size_t ls_smem_bytes(int max_n) {
-  size_t a = GEMM_SMEM_BYTES, b = inv_smem_bytes_host(max_n), c = STREAM_SMEM_BYTES;
+  size_t a = GEMM_SMEM_BYTES, b = lu_smem_bytes_host(max_n), c = STREAM_SMEM_BYTES;
   size_t m = a > b ? a : b;
   return m > c ? m : c;
 }

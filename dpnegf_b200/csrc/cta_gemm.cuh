@@ -15,9 +15,14 @@
 
 namespace negf {
 
-constexpr int GT_M = 64, GT_N = 64, GT_K = 16;
-constexpr int PITCH_MK = GT_K + 4;  // [64 rows][16 k] tiles (pitch = 4 mod 8)
-constexpr int PITCH_KN = GT_N + 2;  // [16 k][64 cols] tiles (pitch = 2 mod 8)
+#ifndef NEGF_GT_K
+#define NEGF_GT_K 16
+#endif
+constexpr int GT_M = 64, GT_N = 64, GT_K = NEGF_GT_K;
+static_assert(GT_K == 16 || GT_K == 32, "k slab of 16 or 32");
+constexpr int PITCH_MK = GT_K + 4;  // [64 rows][GT_K k] tiles (pitch = 4 mod 8)
+constexpr int PITCH_KN = GT_N + 2;  // [GT_K k][64 cols] tiles (pitch = 2 mod 8)
+constexpr int GT_LOADS = GT_M * GT_K / 256;  // 16-byte copies per thread per operand tile
 constexpr int GT_TILE = (GT_M * PITCH_MK > GT_K * PITCH_KN) ? GT_M * PITCH_MK : GT_K * PITCH_KN;
 constexpr int GT_STAGES = 3;
 constexpr int GEMM_SMEM_BYTES = 2 * GT_STAGES * GT_TILE * (int)sizeof(cplx);  // stages x (A,B)
@@ -58,7 +63,7 @@ NEGF_DEV int b_idx(int k, int n) { return OP == OP_C ? n * PITCH_MK + k : k * PI
 template <int OP>
 NEGF_DEV void load_a_tile(cplx* sA, const GemmArgs& g, int m0, int k0, int tid) {
 #pragma unroll
-  for (int s = 0; s < 4; ++s) {
+  for (int s = 0; s < GT_LOADS; ++s) {
     int e = tid + s * CTA_THREADS;
     if (OP == OP_C) {  // stored X is K x M: tile rows k, cols m
       int r = e >> 6, c = e & 63;
@@ -67,7 +72,7 @@ NEGF_DEV void load_a_tile(cplx* sA, const GemmArgs& g, int m0, int k0, int tid) 
       const cplx* src = v ? g.A + (int64_t)k * g.lda + m : g.A;
       cp_async16(sA + r * PITCH_KN + c, src, v);
     } else {  // stored A is M x K: tile rows m, cols k
-      int r = e >> 4, c = e & 15;
+      int r = e / GT_K, c = e % GT_K;
       int m = m0 + r, k = k0 + c;
       bool v = (m < g.M) && (k < g.K);
       const cplx* src = v ? g.A + (int64_t)m * g.lda + k : g.A;
@@ -80,10 +85,10 @@ NEGF_DEV void load_a_tile(cplx* sA, const GemmArgs& g, int m0, int k0, int tid) 
 template <int OP>
 NEGF_DEV void load_b_tile(cplx* sB, const GemmArgs& g, int k0, int n0, int tid) {
 #pragma unroll
-  for (int s = 0; s < 4; ++s) {
+  for (int s = 0; s < GT_LOADS; ++s) {
     int e = tid + s * CTA_THREADS;
     if (OP == OP_C) {  // stored X is N x K: tile rows n, cols k
-      int r = e >> 4, c = e & 15;
+      int r = e / GT_K, c = e % GT_K;
       int n = n0 + r, k = k0 + c;
       bool v = (n < g.N) && (k < g.K);
       const cplx* src = v ? g.B + (int64_t)n * g.ldb + k : g.B;

@@ -36,9 +36,9 @@ constexpr int INV_OB = 128;      // default outer block (columns) of the two-lev
 constexpr int INV_OB_MAX = 512;  // widest outer block (one block: no outer update for n <= 512)
 
 // Shared memory: panel, R tiles, pivot row and multiplier columns, then the
-// integer maps (piv, pinv, reductions).  With the tensor-core outer update
-// (TC) the maps start above the tcgen05 staging area, which that GEMM
-// overwrites while the update epilogue still reads pinv.
+// integer maps (piv, pinv, reductions).  The maps start above the outer
+// update's GEMM staging area (the DMMA ring, or the tcgen05 planes with TC),
+// which that GEMM overwrites while the update epilogue still reads pinv.
 template <int NB>
 struct InvLayout {
   static constexpr int PP = NB + 4;  // panel pitch (= 4 mod 8: conflict-free A fragments)
@@ -49,18 +49,20 @@ struct InvLayout {
     return b + 2 * (size_t)rows(n) * sizeof(double2) + NB * sizeof(double2);  // multiplier columns, spare row
   }
   __host__ __device__ static size_t maps_offset(int n, bool tc) {
-    size_t b = panel_bytes(n);
-    return (tc && b < (size_t)TC_SMEM_BYTES) ? (size_t)TC_SMEM_BYTES : b;
+    const size_t b = panel_bytes(n), g = tc ? (size_t)TC_SMEM_BYTES : (size_t)GEMM_SMEM_BYTES;
+    return b < g ? g : b;
   }
   __host__ __device__ static size_t bytes(int n, bool tc) {
     return maps_offset(n, tc) + (size_t)(2 * n + 64) * sizeof(int) + 16 * sizeof(double);
   }
 };
 
-// Largest footprint over every block size up to max_n: blocks up to 256 use
-// 32-wide panels, larger ones 16-wide panels, and a device may mix both.
+// Largest footprint over every block size up to max_n: blocks of 65..256 use
+// 32-wide panels, the others 16-wide panels, and a device may mix both.
 inline size_t inv_smem_bytes_host(int max_n, bool tc = false) {
   size_t a = InvLayout<32>::bytes(max_n < 256 ? max_n : 256, tc);
+  const size_t s = InvLayout<16>::bytes(max_n < 64 ? max_n : 64, tc);
+  if (s > a) a = s;
   if (max_n > 256) {
     const size_t b = InvLayout<16>::bytes(max_n, tc);
     if (b > a) a = b;
@@ -363,7 +365,10 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
 template <bool G3 = true, bool TC = false>
 NEGF_DEV int cta_inverse(cplx* W, int64_t ldw, int n, cplx* G, int64_t ldg, char* smem_raw, PhaseClock* pc,
                          cplx* snap, int ob = INV_OB) {
-  if (n <= 256) return cta_inverse_nb<32, 1, G3, TC>(W, ldw, n, G, ldg, smem_raw, pc, snap, ob);
+  // 16-wide panels for small blocks (the block inverse's 64-wide leaves): a column step's
+  // latency chain is shorter, measured 22 % faster at n = 64 (8 % at n = 128, where the
+  // rank-16 updates start to cost more)
+  if (n > 64 && n <= 256) return cta_inverse_nb<32, 1, G3, TC>(W, ldw, n, G, ldg, smem_raw, pc, snap, ob);
   return cta_inverse_nb<16, 2, G3, TC>(W, ldw, n, G, ldg, smem_raw, pc, snap, ob);
 }
 

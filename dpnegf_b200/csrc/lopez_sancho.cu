@@ -16,7 +16,8 @@
 //   g_s = (zS - eps_s)^-1, accepted when
 //     max |(zS - H - (z s01 - h01) g_s (z s10 - h10)) g_s - I| < 3e-5
 //     (warning status above 1e-8)
-// Complex products use the conventional 4M form: the doubling iteration
+// The four products of a step are one GEMM of the stacked [alpha; beta] with
+// [Xa Xb].  Complex products use the conventional 4M form: the doubling iteration
 // amplifies the looser componentwise error of Gauss/3M products to ~1e-9 on
 // g_s at ill-conditioned energies.
 // and the self-energy product of selfEnergy (:73-86):
@@ -112,10 +113,11 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
   const cplx ONE = cmk(1.0, 0.0);
   cplx* b_[LS_NBUF];
   for (int i = 0; i < LS_NBUF; ++i) b_[i] = slot + i * mn2;
-  cplx *eps = b_[0], *epss = b_[1], *alpha = b_[2], *beta = b_[3], *alpha2 = b_[4], *beta2 = b_[5];
-  // Xab = [Xa Xb] (n x 2n, row stride 2n) spans b_[8] and b_[9]; b_[7] is spare
-  cplx *A = b_[6], *Xab = b_[8], *T = b_[10], *gsb = b_[11], *t1 = b_[12], *t2 = b_[13];
-  cplx *Xa = Xab, *Xb = Xab + n;
+  // [alpha; beta] stacked (2n x n, row stride n) in the pair b_[2..3]; the next step's in b_[4..5]
+  cplx *eps = b_[0], *epss = b_[1], *AB = b_[2], *AB2 = b_[4];
+  // Xab = [Xa Xb] (n x 2n, row stride 2n) spans b_[8..9]; Pm = [alpha; beta][Xa Xb] (2n x 2n) spans
+  // b_[10..13], whose blocks serve as T, gsb, t1, t2 once the doubling is done
+  cplx *A = b_[6], *Xab = b_[8], *Pm = b_[10], *T = b_[10], *gsb = b_[11], *t1 = b_[12], *t2 = b_[13];
   cplx *Ya = b_[8], *Yb = b_[9];  // separate n x n work blocks once the doubling is done
   const int n2c = 2 * n;
   int bad = 0;
@@ -126,8 +128,8 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
   };
 
   // alpha = h10 - z s10 = h01^H - z s01^H ; beta = h01 - z s01 ; eps = eps_s = H
-  form_herm_shift(alpha, h01, s01, z, n);
-  cta_shift_form(beta, h01, s01, z, ONE, (int)n2, smem);
+  form_herm_shift(AB, h01, s01, z, n);
+  cta_shift_form(AB + n2, h01, s01, z, ONE, (int)n2, smem);
   cta_shift_form(eps, H, nullptr, cmk(0.0, 0.0), ONE, (int)n2, smem);
   cta_shift_form(epss, H, nullptr, cmk(0.0, 0.0), ONE, (int)n2, smem);
 
@@ -139,32 +141,28 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
     cta_shift_form(A, eps, S, z, cmk(-1.0, 0.0), (int)n2, smem);
     for (int e = threadIdx.x; e < n2; e += CTA_THREADS) {
       const int i = e / n, j = e % n;
-      Xab[(int64_t)i * n2c + j] = alpha[e];
-      Xab[(int64_t)i * n2c + n + j] = beta[e];
+      Xab[(int64_t)i * n2c + j] = AB[e];
+      Xab[(int64_t)i * n2c + n + j] = AB[n2 + e];
     }
     __syncthreads();
     bad |= cta_lu_solve(A, n, n, Xab, n2c, n2c, smem_raw);
-    gemm_ls<OP_N, OP_N>(smem, n, n, n, beta, n, Xa, n2c, T, n);  // beta Xa
-    // eps_s += beta Xa ; eps += beta Xa (then + alpha Xb below)
-#pragma unroll 4
-    for (int e = threadIdx.x; e < n2; e += CTA_THREADS) {
-      epss[e] = cadd(epss[e], T[e]);
-      eps[e] = cadd(eps[e], T[e]);
-    }
-    __syncthreads();
-    gemm_ls<OP_N, OP_N>(smem, n, n, n, alpha, n, Xb, n2c, eps, n, eps, n);  // eps += alpha Xb
-    gemm_ls<OP_N, OP_N>(smem, n, n, n, alpha, n, Xa, n2c, alpha2, n);        // alpha <- alpha Xa
-    gemm_ls<OP_N, OP_N>(smem, n, n, n, beta, n, Xb, n2c, beta2, n);          // beta <- beta Xb
-    cplx* t = alpha; alpha = alpha2; alpha2 = t;
-    t = beta; beta = beta2; beta2 = t;
+    // the four products of the step in one GEMM: [alpha; beta] [Xa Xb] = [[aXa, aXb], [bXa, bXb]]
+    gemm_ls<OP_N, OP_N>(smem, n2c, n2c, n, AB, n, Xab, n2c, Pm, n2c);
+    // eps = eps + alpha Xb + beta Xa;  eps_s += beta Xa;  alpha <- alpha Xa;  beta <- beta Xb
     double m = 0.0;
-#pragma unroll 4
     for (int e = threadIdx.x; e < n2; e += CTA_THREADS) {
-      cplx a = alpha[e], b = beta[e];
-      double v = hypot(a.x, a.y) + hypot(b.x, b.y);
+      const int64_t i = e / n, j = e % n;
+      const cplx aXa = Pm[i * n2c + j], aXb = Pm[i * n2c + n + j];
+      const cplx bXa = Pm[(n + i) * n2c + j], bXb = Pm[(n + i) * n2c + n + j];
+      eps[e] = cadd(cadd(eps[e], aXb), bXa);
+      epss[e] = cadd(epss[e], bXa);
+      AB2[e] = aXa;
+      AB2[n2 + e] = bXb;
+      const double v = hypot(aXa.x, aXa.y) + hypot(bXb.x, bXb.y);
       m = (v == v) ? fmax(m, v) : INFINITY;
     }
-    m = cta_max(m, red);
+    cplx* t = AB; AB = AB2; AB2 = t;
+    m = cta_max(m, red);  // begins with a barrier: the pass above is complete
     if (m < P.tol) { converged = true; break; }
     if (!isfinite(m)) break;
   }

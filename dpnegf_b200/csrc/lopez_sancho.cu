@@ -121,10 +121,14 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
   cplx *Ya = b_[8], *Yb = b_[9];  // separate n x n work blocks once the doubling is done
   const int n2c = 2 * n;
   int bad = 0;
-  // out = I (n x n)
-  auto set_eye = [&](cplx* out) {
-    for (int e = threadIdx.x; e < n2; e += CTA_THREADS) out[e] = cmk(e / n == e % n ? 1.0 : 0.0, 0.0);
+  // out = W^-1 (n x n) by the LU solve against I (numpy.linalg.inv's route); W is destroyed
+  auto lu_inverse = [&](cplx* W, cplx* out) {
+    int f = cta_lu_factor(W, n, n, smem_raw);
+    const int* perm = cta_lu_perm(smem_raw, n);
+    for (int e = threadIdx.x; e < n2; e += CTA_THREADS) out[e] = cmk(perm[e / n] == e % n ? 1.0 : 0.0, 0.0);
     __syncthreads();
+    cta_lu_trsolve(W, n, n, out, n, n, smem_raw);
+    return f;
   };
 
   // alpha = h10 - z s10 = h01^H - z s01^H ; beta = h01 - z s01 ; eps = eps_s = H
@@ -139,13 +143,18 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
     it_n = iter;
     // A = zS - eps;  [Xa Xb] = A^-1 [alpha beta]
     cta_shift_form(A, eps, S, z, cmk(-1.0, 0.0), (int)n2, smem);
-    for (int e = threadIdx.x; e < n2; e += CTA_THREADS) {
-      const int i = e / n, j = e % n;
-      Xab[(int64_t)i * n2c + j] = AB[e];
-      Xab[(int64_t)i * n2c + n + j] = AB[n2 + e];
+    bad |= cta_lu_factor(A, n, n, smem_raw);
+    {  // the right-hand sides [alpha beta] in the pivoted row order
+      const int* perm = cta_lu_perm(smem_raw, n);
+      for (int e = threadIdx.x; e < n2; e += CTA_THREADS) {
+        const int i = e / n, j = e % n;
+        const int64_t src = (int64_t)perm[i] * n + j;
+        Xab[(int64_t)i * n2c + j] = AB[src];
+        Xab[(int64_t)i * n2c + n + j] = AB[n2 + src];
+      }
+      __syncthreads();
     }
-    __syncthreads();
-    bad |= cta_lu_solve(A, n, n, Xab, n2c, n2c, smem_raw);
+    cta_lu_trsolve(A, n, n, Xab, n2c, n2c, smem_raw);
     // the four products of the step in one GEMM: [alpha; beta] [Xa Xb] = [[aXa, aXb], [bXa, bXb]]
     gemm_ls<OP_N, OP_N>(smem, n2c, n2c, n, AB, n, Xab, n2c, Pm, n2c);
     // eps = eps + alpha Xb + beta Xa;  eps_s += beta Xa;  alpha <- alpha Xa;  beta <- beta Xb
@@ -173,10 +182,9 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
     st = NEGF_ERR_LS_NOT_CONVERGED;
   } else {
     cplx* gs = it.gs ? reinterpret_cast<cplx*>(it.gs) : gsb;
-    // g_s = (zS - eps_s)^-1 by the LU solve against I (numpy.linalg.inv's route)
+    // g_s = (zS - eps_s)^-1
     cta_shift_form(A, epss, S, z, cmk(-1.0, 0.0), (int)n2, smem);
-    set_eye(gs);
-    bad |= cta_lu_solve(A, n, n, gs, n, n, smem_raw);
+    bad |= lu_inverse(A, gs);
     // residual: (zS - H - (z s01 - h01) g_s (z s10 - h10)) g_s - I
     // z s01 - h01
 #pragma unroll 4
@@ -218,8 +226,7 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
       } else {
         // bulk form: Sigma = (E S - H) - g_s^-1
         cta_shift_form(A, gs, nullptr, cmk(0.0, 0.0), ONE, (int)n2, smem);
-        set_eye(Ya);
-        bad |= cta_lu_solve(A, n, n, Ya, n, n, smem_raw);
+        bad |= lu_inverse(A, Ya);
 #pragma unroll 4
         for (int e = threadIdx.x; e < n2; e += CTA_THREADS) sig[e] = csub(csub(cmul(E, S[e]), H[e]), Ya[e]);
         __syncthreads();

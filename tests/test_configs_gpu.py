@@ -136,8 +136,14 @@ def test_config4_gradient_matches_finite_differences():
     kT = 25 meV (trapezoid weights) + the occupied summed onsite density, with both
     self-energies from the GPU decimation of the edge-pair leads (differentiable through the
     decimation fixed point).  The gradient from one adjoint launch (plus the lead chain rule)
-    against central differences with h = 1e-6 on 64 random entries: 56 of the device blocks,
-    8 of the leads' inter-layer couplings."""
+    against central differences with h = 1e-6 on 64 random entries: 56 of the device blocks
+    (leads at eta = 1e-5) and 8 of the leads' inter-layer couplings.
+
+    The lead entries are checked with the leads broadened to 1e-3: at 1e-5 the self-energies
+    have features of width 1e-5 at the leads' band edges (about 20 in this window), so a step of
+    1e-6 in a coupling moves them by a tenth of their width and the difference quotient itself is
+    off by up to ~1e-3 relative; at 1e-3 the same code path (decimation, implicit-function
+    adjoint, lead chain rule) is checked to the tolerance of the device entries."""
     from dpnegf_b200 import workload
     from dpnegf_b200.adjoint import lead_self_energy, transmission_dos
     b, L, nE = 96, 32, 1024
@@ -152,15 +158,12 @@ def test_config4_gradient_matches_finite_differences():
     wI = ((fL - fR) * tw).cuda()
     wn = (0.5 * (fL + fR) * tw).cuda()
     Ez = E.to(torch.complex128).cuda()
-    eta, eta_lead = 1e-5, 1e-5
+    eta = 1e-5
     names = ("hd", "hu", "hl", "sd", "su", "sl")
-    blocks = {k: [x.cuda().requires_grad_(True) for x in getattr(d, k)] for k in names}
-    lead = {s: {k: getattr(ld, k).cuda() for k in ("hL", "hLL", "sL", "sLL", "hDL", "sDL")}
-            for s, ld in (("L", d.lead_L), ("R", d.lead_R))}
-    for s in ("L", "R"):
-        lead[s]["hLL"].requires_grad_(True)
+    rng = np.random.default_rng(7)
+    h = 1e-6
 
-    def sigmas(ld):
+    def sigmas(ld, eta_lead):
         return {s: lead_self_energy(ld[s]["hL"], ld[s]["hLL"], ld[s]["sL"], ld[s]["sLL"], E, eta_lead,
                                     ld[s]["hDL"], ld[s]["sDL"]) for s in ("L", "R")}
 
@@ -169,47 +172,57 @@ def test_config4_gradient_matches_finite_differences():
                                 sig["R"], eta=eta)
         return (wI * T).sum() + (wn * D).sum()
 
-    Lv = loss(blocks, sigmas(lead))
-    L0 = float(Lv.item())
-    Lv.backward()
+    def grads(eta_lead):
+        blocks = {k: [x.cuda().requires_grad_(True) for x in getattr(d, k)] for k in names}
+        lead = {s: {k: getattr(ld, k).cuda() for k in ("hL", "hLL", "sL", "sLL", "hDL", "sDL")}
+                for s, ld in (("L", d.lead_L), ("R", d.lead_R))}
+        for s in ("L", "R"):
+            lead[s]["hLL"].requires_grad_(True)
+        Lv = loss(blocks, sigmas(lead, eta_lead))
+        Lv.backward()
+        return blocks, lead, float(Lv.item())
+
     checks = []
-    rng = np.random.default_rng(7)
-    h = 1e-6
-    picks = []
-    for _ in range(56):
-        name = names[rng.integers(len(names))]
-        q = int(rng.integers(len(blocks[name])))
-        X = blocks[name][q]
-        picks.append(("dev", name, q, int(rng.integers(X.shape[0])), int(rng.integers(X.shape[1]))))
-    for s in ("L", "R"):
-        for _ in range(4):
-            picks.append(("lead", s, 0, int(rng.integers(b)), int(rng.integers(b))))
-    worst = 0.0
+    # device entries, leads at eta = 1e-5
+    blocks, lead, L0 = grads(1e-5)
     with torch.no_grad():
         base = {k: [x.detach().clone() for x in v] for k, v in blocks.items()}
-        lbase = {s: {k: v.detach().clone() for k, v in lead[s].items()} for s in lead}
-        sig0 = sigmas(lbase)  # the device entries leave the self-energies unchanged
-        for kind, name, q, i, j in picks:
+        sig0 = sigmas({s: {k: v.detach() for k, v in lead[s].items()} for s in lead}, 1e-5)
+        for _ in range(56):
+            name = names[rng.integers(len(names))]
+            q = int(rng.integers(len(base[name])))
+            i, j = int(rng.integers(base[name][q].shape[0])), int(rng.integers(base[name][q].shape[1]))
             ph = np.exp(2j * np.pi * rng.random())  # a random complex direction of unit modulus
 
-            def shifted(sgn):  # loss at the entry moved by sgn * h along ph
+            def shifted(sgn):
                 bl = {k: list(v) for k, v in base.items()}
-                if kind == "dev":
-                    bl[name][q] = bl[name][q].clone()
-                    bl[name][q][i, j] += sgn * h * ph
-                    return loss(bl, sig0).item()
-                ld = {s: dict(v) for s, v in lbase.items()}
-                ld[name]["hLL"] = ld[name]["hLL"].clone()
-                ld[name]["hLL"][i, j] += sgn * h * ph
-                return loss(bl, sigmas(ld)).item()
+                bl[name][q] = bl[name][q].clone()
+                bl[name][q][i, j] += sgn * h * ph
+                return loss(bl, sig0).item()
 
-            fd = (shifted(1) - shifted(-1)) / (2 * h)
-            g = (blocks[name][q].grad if kind == "dev" else lead[name]["hLL"].grad)[i, j].item()
-            ad = g.real * ph.real + g.imag * ph.imag  # directional derivative, torch's convention
-            checks.append((kind, name, q, i, j, fd, ad))
+            g = blocks[name][q].grad[i, j].item()
+            checks.append(("dev", name, q, i, j, (shifted(1) - shifted(-1)) / (2 * h),
+                           g.real * ph.real + g.imag * ph.imag))
+    # lead couplings, leads at eta = 1e-3
+    blocks, lead, _ = grads(1e-3)
+    with torch.no_grad():
+        base = {k: [x.detach() for x in v] for k, v in blocks.items()}
+        lbase = {s: {k: v.detach().clone() for k, v in lead[s].items()} for s in lead}
+        for side in ("L", "R"):
+            for _ in range(4):
+                i, j = int(rng.integers(b)), int(rng.integers(b))
+                ph = np.exp(2j * np.pi * rng.random())
+
+                def shifted(sgn):
+                    ld = {s: dict(v) for s, v in lbase.items()}
+                    ld[side]["hLL"] = ld[side]["hLL"].clone()
+                    ld[side]["hLL"][i, j] += sgn * h * ph
+                    return loss(base, sigmas(ld, 1e-3)).item()
+
+                g = lead[side]["hLL"].grad[i, j].item()
+                checks.append(("lead", side, 0, i, j, (shifted(1) - shifted(-1)) / (2 * h),
+                               g.real * ph.real + g.imag * ph.imag))
     gmax = max(abs(c[6]) for c in checks)
     for kind, name, q, i, j, fd, ad in checks:
         tol = 1e-5 * gmax + 1e-4 * abs(ad)
-        worst = max(worst, abs(fd - ad) / tol)
         assert abs(fd - ad) <= tol, (kind, name, q, i, j, fd, ad, gmax, L0)
-    assert worst <= 1.0

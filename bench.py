@@ -301,6 +301,12 @@ def current_density_leg(torch, rgf_plan, workload, eta):
                                         adjoint_w=wI, adjoint_w_dos=wn, precision=prec))
         out[prec] = {"forward_value": nE / (tf * 1e-3), "grad_value": nE / (tg * 1e-3), "grad_over_forward": tg / tf,
                      "unit": UNIT}
+        if prec == "fp64":  # the config's "checkpoints every 6 blocks": g_q kept for q = 0, 6, ... only
+            tc = timed(lambda: rgf_plan.run(geom, [Ez], [seL], [seR], eta=eta, outputs=(), check=False,
+                                            adjoint_w=wI, adjoint_w_dos=wn, precision=prec, checkpoint=6))
+            out[prec]["checkpoint6"] = {"grad_value": nE / (tc * 1e-3), "grad_over_forward": tc / tf,
+                                        "g_storage_blocks_per_slot": f"{(L + 5) // 6 + 6} of {L} (g and its "
+                                                                     f"z-tangent each)"}
     out["note"] = ("config-4 loss I + n (Landauer current by trapezoid weights at V=0.3 V, kT=25 meV, plus the "
                    "occupied summed onsite density); grad_value = energy points/s of T plus the full gradient "
                    "from one adjoint launch (T adjoint + z-tangent density pass); grad_over_forward = that "

@@ -113,7 +113,8 @@ class NegfRgfProblem(ctypes.Structure):
         ("inv_ob", ctypes.c_int32),
         ("s_out", ctypes.c_void_p),
         ("inv_mode", ctypes.c_int32),
-        ("pad1", ctypes.c_int32),
+        ("ckpt", ctypes.c_int32),
+        ("ckpt_blocks", ctypes.c_int32),
     ]
 
 

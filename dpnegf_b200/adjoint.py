@@ -10,8 +10,13 @@ device and accumulates, for the loss L = sum_E w_E T(E) with w = dL/dT,
 plus the explicit Gamma terms of the self-energies, dT/dSigma_L = -2i G_1N
 Gamma_R G_1N^H (and its mirror for Sigma_R).  G_qN comes from the backward
 sweep, the first block row from G_1p = P_p G_pp with P_{p+1} = P_p g_p U_p.
-The re-sweep keeps nothing from the forward call (the extreme of
-checkpointing); one backward costs about 1.7x a forward sweep.
+The re-sweep keeps nothing from the forward call; one backward costs about
+1.7x a forward sweep.  Inside the adjoint launch every left-connected g_q of
+the item stays in the item's scratch slot, or, with ``checkpoint=s`` on
+``transmission_and_grad`` / ``rgf_plan.run``, only g_0, g_s, g_2s, ... and one
+segment of s blocks, each segment recomputed from its checkpoint when the
+backward sweep and the adjoint pass reach it (sqrt(K) checkpointing for
+blocks too large to keep).
 
 ``transmission_dos(...)`` returns T(E) and DOS(E) (the reference's _cal_dos_,
 device_property.py:408-439: -(2/pi) Im Tr[G S] with the block-tridiagonal
@@ -141,7 +146,7 @@ def transmission_and_grad(hd: Sequence[torch.Tensor], hu: Sequence[torch.Tensor]
                           sd: Sequence[torch.Tensor], su: Sequence[torch.Tensor], sl: Sequence[torch.Tensor],
                           energy: torch.Tensor, left_se: torch.Tensor, right_se: torch.Tensor,
                           weights: torch.Tensor, eta: float = 0.0, E_ref: float = 0.0, precision: str = "fp64",
-                          refine: bool = False, dos_weights=None):
+                          refine: bool = False, dos_weights=None, checkpoint=0):
     """T(E) and the gradient of L = sum_E w_E T(E) for weights known in advance, in one launch.
 
     The adjoint pass sweeps the device itself and reduces T(E) on the way, so
@@ -155,7 +160,10 @@ def transmission_and_grad(hd: Sequence[torch.Tensor], hu: Sequence[torch.Tensor]
     ``transmission`` gives for ``(w * T).sum()``.  ``refine`` refines the
     column G_{:,N} (mixed precision) before T and the gradient are formed.
     ``dos_weights`` ([B]) add the gradient of sum_E wd_E DOS(E) (the summed
-    onsite density for occupation x quadrature weights) to the same launch."""
+    onsite density for occupation x quadrature weights) to the same launch.  ``checkpoint``
+    (an interval s, or "sqrt") keeps only every s-th left-connected block of the forward sweep
+    and recomputes the others segment by segment (rgf_plan.run), for devices whose full set of
+    blocks does not fit the per-SM scratch."""
     K = len(hd)
     if not (len(sd) == K and len(hu) == len(hl) == len(su) == len(sl) == K - 1):
         raise ValueError("inconsistent block lists")
@@ -174,7 +182,7 @@ def transmission_and_grad(hd: Sequence[torch.Tensor], hu: Sequence[torch.Tensor]
             raise ValueError(f"{wd.shape[0]} DOS weights for {energy.shape[0]} energies")
     res = rgf_plan.run(geom, [energy], [left_se.detach()], [right_se.detach()], eta=eta, E_ref=E_ref, outputs=(),
                        adjoint_w=w, adjoint_w_dos=wd, precision=precision, refine=refine,
-                       refine_steps=3 if refine else 1)
+                       refine_steps=3 if refine else 1, checkpoint=checkpoint)
     return res.trans.clone(), res.grads
 
 

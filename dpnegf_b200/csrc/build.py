@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 ROOT = os.path.dirname(PKG)
 OUT = os.path.join(PKG, "libnegf_b200.so")
-SOURCES = ["rgf.cu", "rgf_noalloc.cu", "lopez_sancho.cu"]
+SOURCES = ["rgf.cu", "rgf_mx.cu", "rgf_noalloc.cu", "lopez_sancho.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-v"]
 
@@ -38,16 +38,33 @@ def stale():
 
 
 def build(force=False, verbose=False):
+    """Compile every source to an object in parallel, then link the shared library."""
     if not force and not stale():
         return OUT
-    cmd = [_nvcc()] + NVCC_FLAGS + ["-I", os.path.join(ROOT, "include"), "-o", OUT + ".tmp"]
-    cmd += [os.path.join(HERE, s) for s in SOURCES]
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    procs = []
+    for src in SOURCES:
+        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+        cmd = [_nvcc()] + flags + ["-I", os.path.join(ROOT, "include"), "-c", os.path.join(HERE, src), "-o", obj]
+        procs.append((src, obj, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+    objs, log = [], ""
+    for src, obj, pr in procs:
+        out, err = pr.communicate()
+        log += out + err
+        if pr.returncode != 0:
+            sys.stderr.write(out + err)
+            raise RuntimeError(f"nvcc failed on {src}")
+        objs.append(obj)
+    cmd = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC",
+           "-o", OUT + ".tmp"] + objs
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed")
+        raise RuntimeError("nvcc link failed")
     if verbose:
-        sys.stdout.write(r.stderr)
+        sys.stdout.write(log)
     os.replace(OUT + ".tmp", OUT)
     return OUT
 

@@ -209,7 +209,7 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
         s_in: Optional[List[List[Optional[torch.Tensor]]]] = None,
         s_out: Optional[List[List[Optional[torch.Tensor]]]] = None,
         n_slots=None, check=True, stream=None, phase=False, events=None, adjoint_w=None, adjoint_w_dos=None,
-        precision="fp64", refine=False, refine_steps=1, defer=False, inv_ob=None, inverse=None):
+        precision="fp64", refine=False, refine_steps=1, defer=False, inv_ob=None, inverse=None, checkpoint=0):
     """Run the batched sweep.
 
     ``energies[d]`` is a 1-D tensor of B_d energies for device d; ``se_l[d]``
@@ -243,6 +243,11 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     ``inv_ob`` is the inverse's outer block width (32..512); by default the
     autotuned value for this GPU, block size and precision (``autotune.lookup``),
     else 128.
+    ``checkpoint`` (adjoint only): 0 keeps every left-connected g_q of an item in its scratch slot;
+    s > 0 keeps g_0, g_s, g_2s, ... and one segment of s blocks, recomputing each segment from its
+    checkpoint when the backward sweep and the adjoint pass reach it (``"sqrt"``: s = ceil(sqrt(K))),
+    so the g storage per slot is (ceil(K/s) + s) max_n^2 instead of sum n_q^2 (twice that with
+    ``adjoint_w_dos``, whose z-tangents are checkpointed alike); results are identical.
     ``defer=True`` builds everything but launches nothing and returns an
     ``RgfPlan``: its ``launch()`` re-runs the sweep on the same descriptors,
     scratch and output tensors (a queue reset and one kernel, so it can be
@@ -297,6 +302,16 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
         if not trans:
             raise ValueError("refine improves T(E): it needs trans=True")
         flags |= _lib.REFINE
+    ckpt = 0
+    if checkpoint:
+        if not adjoint:
+            raise ValueError("checkpoint applies to the adjoint pass (adjoint_w / adjoint_w_dos)")
+        if refine or lesser or greater or "gr_left" in outputs:
+            raise ValueError("checkpointing does not combine with refine, lesser, greater or gr_left outputs")
+        K0 = int(geom.devs[0]["n_blocks"])
+        ckpt = int(np.ceil(np.sqrt(K0))) if checkpoint == "sqrt" else int(checkpoint)
+        if ckpt < 1:
+            raise ValueError(f"checkpoint interval must be >= 1, not {checkpoint!r}")
 
     blocks = geom.blocks.copy()
     devs = geom.devs.copy()
@@ -456,6 +471,9 @@ def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.
     if refine or adjoint:
         prob.col_slab = max(int(geom.col_slab), 1)
     prob.refine_steps = int(refine_steps)
+    if ckpt:
+        prob.ckpt = ckpt
+        prob.ckpt_blocks = int(geom.devs[0]["n_blocks"])
     if inv_ob is None or inverse is None:
         from . import autotune
         tuned = autotune.lookup(geom.max_n, precision)

@@ -164,7 +164,14 @@ typedef struct NegfRgfProblem {
                                which the retarded problem guarantees for eta > 0 (zS - H - Sigma - L g U
                                has a positive-definite imaginary part when H is Hermitian, S positive
                                definite and Im Sigma <= 0) */
-  int32_t pad1;
+  int32_t ckpt;             /* NEGF_ADJOINT: 0 keeps every left-connected g_q (and, with NEGF_ADJ_DOS, its
+                               z-tangent) for the whole item; s > 0 keeps only g_q for q = 0, s, 2s, ...
+                               plus one segment of s blocks, and recomputes each segment from its
+                               checkpoint when the backward sweep and the adjoint pass reach it (sqrt(K)
+                               checkpointing: g storage (ceil(K/s) + s) max_n^2 instead of sum n_q^2, at
+                               the cost of up to two extra forward sweeps).  Not with gr_left outputs,
+                               lesser, greater or refinement */
+  int32_t ckpt_blocks;      /* with ckpt > 0: the device's block count K (sizes the checkpoint area) */
 } NegfRgfProblem;
 
 /* ---- Lopez-Sancho lead decimation ------------------------------------ */

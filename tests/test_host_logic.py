@@ -68,3 +68,23 @@ def test_density_onsite_matches_reference():
     DM = torch.as_tensor(g["DM"])
     np.testing.assert_array_equal(oz.get_density_onsite(dp, DM).numpy(), g["out/matrix"])
     np.testing.assert_array_equal(oz.get_density_onsite(dp, DM.diag() * 2).numpy(), g["out/vector"])
+
+
+def test_checkpointing_shrinks_the_rgf_slot():
+    """With sqrt(K) checkpointing the g and z-tangent slabs of an adjoint slot shrink from
+    sum n_q^2 to (ceil(K/s) + s) max_n^2 each (host-side sizing, no GPU)."""
+    import ctypes
+    from dpnegf_b200 import _lib
+    K, n = 36, 32
+    sizes = {}
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    lib.negf_rgf_scratch_bytes.restype = ctypes.c_size_t
+    lib.negf_rgf_scratch_bytes.argtypes = [ctypes.POINTER(_lib.NegfRgfProblem)]
+    for ck in (0, 6):
+        p = _lib.NegfRgfProblem()
+        p.max_n, p.max_g_slab, p.n_slots = n, K * n * n, 1
+        p.flags = _lib.ADJOINT | _lib.ADJ_DOS | _lib.TRANS
+        p.col_slab = K * n * n
+        p.ckpt, p.ckpt_blocks = ck, K
+        sizes[ck] = lib.negf_rgf_scratch_bytes(ctypes.byref(p))
+    assert sizes[0] - sizes[6] == 2 * (K - 12) * n * n * 16

@@ -61,6 +61,10 @@ def parse():
     ap.add_argument("--lead-eta", type=float, default=1e-5, help="lead broadening of the 'leads' leg")
     ap.add_argument("--no-leads", action="store_true", help="skip the metric device's lead decimation object")
     ap.add_argument("--uneven-devices", type=int, default=128, help="devices of the 'uneven' leg")
+    ap.add_argument("--uneven-chunk", type=int, default=128, help="devices per launch in the 'uneven' leg")
+    ap.add_argument("--scf-k", type=int, default=8, help="k-points of the 'scf' leg")
+    ap.add_argument("--scf-energies", type=int, default=37, help="energies per k of the 'scf' leg (4096: config)")
+    ap.add_argument("--scf-iters", type=int, default=10, help="timed SCF iterations of the 'scf' leg")
     ap.add_argument("--uneven-precisions", default="fp64,mixed,mixed_refined",
                     help="runs of the 'uneven' leg besides FP64: mixed, mixed_refined")
     ap.add_argument("--inverse", default=None, choices=["gj", "block"],
@@ -325,11 +329,9 @@ def _timed(torch, fn):
     return r, a.elapsed_time(b)
 
 
-# Lead broadening of the synthetic leads (edge blocks of random dense devices): at 1e-5 their
-# decimation on the real axis misses the Lopez-Sancho residual criterion (about 4e-5 against 1e-5
-# near E = 0), which raises as the reference does.
-ETA_LEAD_SYNTH = 1e-3
-ETA_LEAD_NOTE = "lead eta 1e-3 (the random dense leads miss the decimation residual criterion at 1e-5)"
+# Lead broadening of the synthetic leads (edge blocks of random dense devices) in the opt-in legs;
+# the decimation's LU solve keeps the residual check within the reference's bound at 1e-5.
+ETA_LEAD_SYNTH = 1e-5
 
 
 def _ls_flops(n, iters):
@@ -338,8 +340,9 @@ def _ls_flops(n, iters):
     return 8.0 * (7.0 / 3.0 + 4.0) * n ** 3 * iters + 16.0 * n ** 3
 
 
-def _uneven_inputs(torch, n_devices, seed):
-    """Devices with b ~ U{16..256} (step 16) and L ~ U{8..64}, their edge-block leads, and the
+def _uneven_inputs(torch, n_devices, seed, first=0):
+    """Devices first..first+n_devices-1 of the uneven set: b ~ U{16..256} (step 16) and
+    L ~ U{8..64} drawn in device order from one seeded stream, their edge-block leads, and the
     energies: the far pole + 64 Ozaki poles at kT = 25 meV + 256 Gauss-Legendre points of the
     0.3 V bias window."""
     import numpy as np
@@ -348,10 +351,10 @@ def _uneven_inputs(torch, n_devices, seed):
     from dpnegf_b200.scf import ozaki_weights
     from dpnegf_b200.surface_green import LeadBlocks
     rng = np.random.default_rng(seed)
+    sizes = [(int(rng.integers(1, 17)) * 16, int(rng.integers(8, 65))) for _ in range(first + n_devices)]
     devs, leads, work = [], [], 0.0
-    for d in range(n_devices):
-        b = int(rng.integers(1, 17)) * 16
-        L = int(rng.integers(8, 65))
+    for d in range(first, first + n_devices):
+        b, L = sizes[d]
         dev = workload.random_device(b, L, seed=seed + d)
         devs.append(rgf_plan.DeviceBlocks(dev.hd, dev.hu, dev.hl, dev.sd, dev.su, dev.sl))
         lb = lambda ld: LeadBlocks(ld.hL, ld.hLL, ld.sL, ld.sLL, ld.hDL, ld.sDL)
@@ -417,73 +420,82 @@ def metric_leads_leg(torch, peak, dev, E, eta=1e-5, n_energies=512):
             "workload": f"both edge-pair leads of the b=256 metric device, {len(Es)} energies of [-3, 3] eV"}
 
 
-def uneven_leg(torch, n_devices=128, seed=2024, precisions=("fp64", "mixed", "mixed_refined")):
+def uneven_leg(torch, n_devices=128, seed=2024, precisions=("fp64", "mixed", "mixed_refined"), chunk=128,
+               eta_lead=ETA_LEAD_SYNTH):
     """The uneven batch (``_uneven_inputs``): every lead at every energy in one decimation launch,
-    every (device, energy) item in one persistent sweep (Ozaki.uneven_batch).  FP64, mixed, and
-    mixed + FP64-residual refinement, the mixed runs checked against FP64; the decimation phase
-    also timed alone.  ``n_devices`` of the 512 (the full batch's self-energies alone need about
-    100 GB; it runs as chunks of this size)."""
-    import numpy as np
+    every (device, energy) item in one persistent sweep (Ozaki.uneven_batch), in chunks of
+    ``chunk`` devices (the full batch's self-energies alone need about 100 GB), times summed.
+    FP64, mixed, and mixed + FP64-residual refinement, the mixed runs checked against FP64; the
+    decimation phase also timed alone."""
     from dpnegf_b200.surface_green import LeadArena, self_energies
-    u = _uneven_inputs(torch, n_devices, seed)
-    devs, leads, work, oz = u["devs"], u["leads"], u["work"], u["oz"]
-    kBT, mu_L, vL, vR, fL, fR, z = u["kBT"], u["mu_L"], u["vL"], u["vR"], u["fL"], u["fR"], u["z"]
-    nE = len(z)
-    timed = lambda fn: _timed(torch, fn)
-    # the decimation phase alone: every lead at every energy, one launch
-    arena = LeadArena([ld for pair in leads for ld in pair])
-    ms_lead = timed(lambda: self_energies(arena, np.repeat(np.arange(2 * n_devices), nE),
-                                          np.tile(z, 2 * n_devices), ETA_LEAD_SYNTH))[1]
-    del arena
-    out, ms = {}, {}
     runs = (("fp64", "fp64", False), ("mixed", "mixed", False), ("mixed_refined", "mixed", True))
-    for tag, prec, refine in (r for r in runs if r[0] == "fp64" or r[0] in precisions):
-        kw = dict(vL=vL, vR=vR, fermi_L=fL, fermi_R=fR, eta_lead=ETA_LEAD_SYNTH, eta_device=1e-5, precision=prec,
-                  refine=refine)
-        out[tag], ms[tag] = timed(lambda: oz.uneven_batch(devs, leads, kBT, mu_L, **kw))
-    rel = lambda x, y: float((x - y).abs().max() / max(float(y.abs().max()), 1e-300))
-    items = n_devices * nE
-    res = {"devices": n_devices, "energies_per_device": nE, "items": items,
+    ms = {tag: 0.0 for tag, _, _ in runs}
+    ms_lead, work, items, nE, worst = 0.0, 0.0, 0, 0, {}
+    timed = lambda fn: _timed(torch, fn)
+    for first in range(0, n_devices, chunk):
+        u = _uneven_inputs(torch, min(chunk, n_devices - first), seed, first=first)
+        devs, leads, oz = u["devs"], u["leads"], u["oz"]
+        kBT, mu_L, vL, vR, fL, fR, z = u["kBT"], u["mu_L"], u["vL"], u["vR"], u["fL"], u["fR"], u["z"]
+        nd, nE = len(devs), len(z)
+        arena = LeadArena([ld for pair in leads for ld in pair])
+        ms_lead += timed(lambda: self_energies(arena, np.repeat(np.arange(2 * nd), nE), np.tile(z, 2 * nd),
+                                               eta_lead))[1]
+        del arena
+        out = {}
+        for tag, prec, refine in (r for r in runs if r[0] == "fp64" or r[0] in precisions):
+            kw = dict(vL=vL, vR=vR, fermi_L=fL, fermi_R=fR, eta_lead=eta_lead, eta_device=1e-5, precision=prec,
+                      refine=refine)
+            out[tag], t = timed(lambda: oz.uneven_batch(devs, leads, kBT, mu_L, **kw))
+            ms[tag] += t
+        rel = lambda x, y: float((x - y).abs().max() / max(float(y.abs().max()), 1e-300))
+        for tag in (t for t in ("mixed", "mixed_refined") if t in out):
+            w = worst.setdefault(tag, [0.0, 0.0])
+            w[0] = max(w[0], max(rel(m["n_eq"] + m["n_neq"], f["n_eq"] + f["n_neq"]) for m, f in zip(out[tag], out["fp64"])))
+            w[1] = max(w[1], max(float((m["trans"] - f["trans"]).abs().max()) for m, f in zip(out[tag], out["fp64"])))
+        work += u["work"] * nE
+        items += nd * nE
+        del out, devs, leads, u
+        torch.cuda.empty_cache()
+    res = {"devices": n_devices, "chunk": chunk, "energies_per_device": nE, "items": items,
+           "eta_lead": eta_lead,
            "lead_decimation": {"items": 2 * items, "seconds": ms_lead * 1e-3},
            "fp64": {"value": items / (ms["fp64"] * 1e-3), "unit": "items/s", "seconds": ms["fp64"] * 1e-3,
-                    "sweep_tflops_algorithmic": work * nE / ((ms["fp64"] - ms_lead) * 1e-3) / 1e12}}
-    for tag in (t for t in ("mixed", "mixed_refined") if t in out):
+                    "sweep_tflops_algorithmic": work / ((ms["fp64"] - ms_lead) * 1e-3) / 1e12}}
+    for tag in worst:
         res[tag] = {"value": items / (ms[tag] * 1e-3), "unit": "items/s", "seconds": ms[tag] * 1e-3,
-                    "density_rel_err_vs_fp64": max(rel(m["n_eq"] + m["n_neq"], f["n_eq"] + f["n_neq"])
-                                                   for m, f in zip(out[tag], out["fp64"])),
-                    "t_abs_err_vs_fp64": max(float((m["trans"] - f["trans"]).abs().max())
-                                             for m, f in zip(out[tag], out["fp64"]))}
+                    "density_rel_err_vs_fp64": worst[tag][0], "t_abs_err_vs_fp64": worst[tag][1]}
     return dict(res, **{
-            "note": "one call each (lead decimation + persistent sweep + density reduction), CUDA events; "
-                    "item = (device, energy); lead_decimation = that phase timed alone; sweep_tflops counts "
-                    "72 b^3 L per item over the FP64 call's time less the decimation's; " + ETA_LEAD_NOTE})
+            "note": "per chunk: one call each (lead decimation + persistent sweep + density reduction), CUDA "
+                    "events, summed over chunks; item = (device, energy); lead_decimation = that phase timed "
+                    "alone; sweep_tflops counts 72 b^3 L per item over the FP64 time less the decimation's"})
 
 
-def scf_leg(torch, peak, nk=8):
+def scf_leg(torch, peak, nk=8, n_energies=37, iters=10, eta_lead=ETA_LEAD_SYNTH):
     """b=512, L=40 at ``nk`` k-points (distinct H(k), S(k) realisations, equal weights): lead
-    decimation on 512 x 512 blocks, then 10 timed SCF iterations of damped (0.3) onsite shifts
-    V = 0.5 (n - n0) around one sweep over every (k, energy) item, the iteration replayed as a CUDA
-    graph (scf.ScfLoop); energies per k = far pole + 16 Ozaki poles + 20 bias-window points, so
-    8 k x 37 = 296 items per iteration (two waves of the persistent CTAs).  FP64 and mixed; the
-    mixed density checked against FP64."""
+    decimation on 512 x 512 blocks, then ``iters`` timed SCF iterations of damped (0.3) onsite
+    shifts V = 0.5 (n - n0) around one sweep over every (k, energy) item, the iteration replayed as
+    a CUDA graph (scf.ScfLoop).  Energies per k: the far pole + the Ozaki poles + bias-window
+    points, ``n_energies`` in all (37 = 1 + 16 + 20 by default; 4096 = 1 + 64 + 4031 is the
+    config's count).  FP64 and mixed; the mixed density checked against FP64."""
     import numpy as np
     from dpnegf_b200 import rgf_plan, workload
     from dpnegf_b200.ozaki_res_cal import ozaki_residues
     from dpnegf_b200.scf import ScfLoop, ozaki_weights
     from dpnegf_b200.surface_green import LeadArena, LeadBlocks, self_energies
-    b, L, iters = 512, 40, 10
+    b, L = 512, 40
     devs = [workload.random_device(b, L, seed=512 + k) for k in range(nk)]
     kBT, mu_L, vL, vR = 0.025, 0.0, 0.15, -0.15
-    poles, res = ozaki_residues(16)
+    n_poles = 16 if n_energies <= 37 else 64
+    poles, res = ozaki_residues(n_poles)
     fL = lambda x: 1.0 / (1.0 + torch.exp((x - (mu_L - vL)) / kBT))
     fR = lambda x: 1.0 / (1.0 + torch.exp((x - (mu_L - vR)) / kBT))
-    z, c, w = ozaki_weights(poles.numpy(), res.numpy(), 1e6, 20, kBT, mu_L, vL=vL, vR=vR, fermi_L=fL,
-                            fermi_R=fR)
+    z, c, w = ozaki_weights(poles.numpy(), res.numpy(), 1e6, n_energies - 1 - n_poles, kBT, mu_L, vL=vL, vR=vR,
+                            fermi_L=fL, fermi_R=fR)
     nE = len(z)
     lb = lambda ld: LeadBlocks(ld.hL, ld.hLL, ld.sL, ld.sLL, ld.hDL, ld.sDL)
     arena = LeadArena([lb(ld) for d in devs for ld in (d.lead_L, d.lead_R)])
     ls, t_lead = _timed(torch, lambda: self_energies(arena, np.repeat(np.arange(2 * nk), nE), np.tile(z, 2 * nk),
-                                                     ETA_LEAD_SYNTH))
+                                                     eta_lead))
     sig = [torch.stack(ls.sigma[i * nE:(i + 1) * nE]) for i in range(2 * nk)]
     del arena
     geom = rgf_plan.Geometry([rgf_plan.DeviceBlocks(d.hd, d.hu, d.hl, d.sd, d.su, d.sl) for d in devs])
@@ -501,7 +513,8 @@ def scf_leg(torch, peak, nk=8):
     ach = 72.0 * b ** 3 * L * pts / (ms["fp64"] * 1e-3) / 1e12
     rel = lambda x, y: float((x - y).abs().max() / max(float(y.abs().max()), 1e-300))
     return {"b": b, "L": L, "k_points": nk, "energies_per_k": nE, "iterations": iters,
-            "lead_decimation": {"items": 2 * nk * nE, "seconds": t_lead * 1e-3, "n": b,
+            "lead_decimation": {"items": 2 * nk * nE, "seconds": t_lead * 1e-3, "n": b, "eta": eta_lead,
+                                "status_counts": _status_counts(ls.status),
                                 "mean_iters": float(ls.iters.mean()),
                                 "tflops_algorithmic": float(_ls_flops(float(b), ls.iters.astype(np.float64)).sum())
                                 / (t_lead * 1e-3) / 1e12},
@@ -513,7 +526,7 @@ def scf_leg(torch, peak, nk=8):
                       "V_rel_err_vs_fp64": rel(out["mixed"][0], out["fp64"][0])},
             "note": "energy points = k-points x energies x timed iterations; iterations 0-1 (equilibrium n0, "
                     "graph capture) untimed, then graph replays with the k-summed density reduction and the "
-                    "potential update, CUDA events around them; " + ETA_LEAD_NOTE}
+                    "potential update, CUDA events around them"}
 
 
 def traffic_per_point(b, L):
@@ -837,9 +850,11 @@ def main():
             extra["config3_leads"] = leads_leg(torch, peak, n_devices=args.lead_devices, eta=args.lead_eta)
         if "uneven" in wanted:
             extra["config3_uneven"] = uneven_leg(torch, n_devices=args.uneven_devices,
-                                                 precisions=args.uneven_precisions.split(","))
+                                                 precisions=args.uneven_precisions.split(","),
+                                                 chunk=args.uneven_chunk, eta_lead=args.lead_eta)
         if "scf" in wanted:
-            extra["config5_scf"] = scf_leg(torch, peak)
+            extra["config5_scf"] = scf_leg(torch, peak, nk=args.scf_k, n_energies=args.scf_energies,
+                                           iters=args.scf_iters, eta_lead=args.lead_eta)
 
     # end-to-end through the public API: pinned host inputs, host outputs
     e2e = None

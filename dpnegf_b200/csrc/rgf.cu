@@ -1,5 +1,5 @@
 // The C ABI of the RGF sweep (include/negf_b200.h) and its FP64 kernels; the sweep itself is
-// in rgf_sweep.cuh, the mixed-precision kernels in rgf_mx_*.cu.
+// in rgf_sweep.cuh, the mixed-precision kernel in rgf_mx.cu.
 #include "rgf_sweep.cuh"
 
 namespace negf {

@@ -62,8 +62,55 @@ ITEM_DTYPE = np.dtype([("dev", "<i4"), ("row", "<i4"), ("z_re", "<f8"), ("z_im",
 
 LEAD_DTYPE = np.dtype([("n", "<i4"), ("nc", "<i4"), ("b", "<i4"), ("pad", "<i4"), ("h", "<i8"), ("s", "<i8"),
                        ("h01", "<i8"), ("s01", "<i8"), ("hdl", "<i8"), ("sdl", "<i8")])
-LS_ITEM_DTYPE = np.dtype([("lead", "<i4"), ("pad", "<i4"), ("e_re", "<f8"), ("e_im", "<f8"), ("eta", "<f8"),
+LS_ITEM_DTYPE = np.dtype([("lead", "<i4"), ("mode", "<i4"), ("e_re", "<f8"), ("e_im", "<f8"), ("eta", "<f8"),
                           ("sigma", "<u8"), ("gs", "<u8"), ("out", "<i8")])
+LS_DECIMATE = 0
+LS_SIGMA_FROM_GS = 1
+LEADADJ_ITEM_DTYPE = np.dtype([("e_re", "<f8"), ("e_im", "<f8"), ("gs", "<u8"), ("gsig", "<u8")])
+
+
+class NegfLead(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int32), ("nc", ctypes.c_int32), ("b", ctypes.c_int32), ("pad", ctypes.c_int32),
+                ("h", ctypes.c_int64), ("s", ctypes.c_int64), ("h01", ctypes.c_int64), ("s01", ctypes.c_int64),
+                ("hdl", ctypes.c_int64), ("sdl", ctypes.c_int64)]
+
+
+class NegfGammaSum(ctypes.Structure):
+    _fields_ = [
+        ("g", ctypes.c_void_p),
+        ("g_stride", ctypes.c_int64),
+        ("gamma", ctypes.c_void_p),
+        ("gamma_stride", ctypes.c_int64),
+        ("w", ctypes.c_void_p),
+        ("out", ctypes.c_void_p),
+        ("n_items", ctypes.c_int32),
+        ("n", ctypes.c_int32),
+        ("ldg", ctypes.c_int32),
+        ("c0", ctypes.c_int32),
+        ("k", ctypes.c_int32),
+        ("ldgam", ctypes.c_int32),
+        ("scratch", ctypes.c_void_p),
+        ("scratch_bytes", ctypes.c_size_t),
+    ]
+
+
+class NegfLeadAdjProblem(ctypes.Structure):
+    _fields_ = [
+        ("lead", NegfLead),
+        ("arena", ctypes.c_void_p),
+        ("items", ctypes.c_void_p),
+        ("n_items", ctypes.c_int32),
+        ("form", ctypes.c_int32),
+        ("eta", ctypes.c_double),
+        ("tol", ctypes.c_double),
+        ("max_iter", ctypes.c_int32),
+        ("n_slots", ctypes.c_int32),
+        ("grad", ctypes.c_void_p),
+        ("status", ctypes.c_void_p),
+        ("iters", ctypes.c_void_p),
+        ("scratch", ctypes.c_void_p),
+        ("scratch_bytes", ctypes.c_size_t),
+    ]
 
 
 class NegfLsProblem(ctypes.Structure):
@@ -147,6 +194,14 @@ def load():
     lib.negf_lopez_sancho_scratch_bytes.argtypes = [ctypes.POINTER(NegfLsProblem)]
     lib.negf_lopez_sancho_run.restype = ctypes.c_int
     lib.negf_lopez_sancho_run.argtypes = [ctypes.POINTER(NegfLsProblem), ctypes.c_void_p]
+    lib.negf_gamma_sum_scratch_bytes.restype = ctypes.c_size_t
+    lib.negf_gamma_sum_scratch_bytes.argtypes = [ctypes.POINTER(NegfGammaSum)]
+    lib.negf_gamma_sum_run.restype = ctypes.c_int
+    lib.negf_gamma_sum_run.argtypes = [ctypes.POINTER(NegfGammaSum), ctypes.c_void_p]
+    lib.negf_lead_adjoint_scratch_bytes.restype = ctypes.c_size_t
+    lib.negf_lead_adjoint_scratch_bytes.argtypes = [ctypes.POINTER(NegfLeadAdjProblem)]
+    lib.negf_lead_adjoint_run.restype = ctypes.c_int
+    lib.negf_lead_adjoint_run.argtypes = [ctypes.POINTER(NegfLeadAdjProblem), ctypes.c_void_p]
     _lib = lib
     return lib
 

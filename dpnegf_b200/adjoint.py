@@ -199,9 +199,10 @@ class _LeadSelfEnergyFn(torch.autograd.Function):
     a Stein equation solved by doubling (Lambda += A Lambda B, A <- A^2, B <- B^2:
     2^j terms after j steps, the Lopez-Sancho convergence, since the spectral
     radii of P and Q are below one for eta > 0), and dL/dtheta is the
-    vector-Jacobian product of f at the fixed point with Lambda (torch autograd
-    of one evaluation of f, batched over energies on the GPU), plus the explicit
-    dependence of Sigma on H_DL, S_DL, H and S."""
+    Lambda-weighted derivative of f at the fixed point plus the explicit
+    dependence of Sigma on H_DL, S_DL, H and S.  The whole backward (V, the
+    doubling, the inverse of f's argument and the parameter terms, summed over
+    energies) is one launch of ``negf_lead_adjoint_run``."""
 
     @staticmethod
     def forward(ctx, energies, eta, E_ref, bulk, hL, hLL, sL, sLL, hDL, sDL):
@@ -222,57 +223,18 @@ class _LeadSelfEnergyFn(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, gsig):
+        from .products import lead_adjoint
         energies, gs, hL, hLL, sL, sLL, hDL, sDL = ctx.saved_tensors
-        dev = hL.device
-        E = (energies.to(dev) + ctx.E_ref).view(-1, 1, 1)
-        z = E + 1j * ctx.eta
-        with torch.enable_grad():
-            th = [t.detach().requires_grad_(True) for t in (hL, hLL, sL, sLL)]
-            tHL, tHLL, tSL, tSLL = th
-            dl = [None if t is None else t.detach().requires_grad_(True) for t in (hDL, sDL)]
-            g = gs.detach().requires_grad_(True)
-            if hDL is not None:
-                b = hDL.shape[-1]
-                sdl = dl[1] if dl[1] is not None else torch.zeros_like(dl[0])
-                sig = (E * sdl - dl[0]) @ g[:, :b, :b] @ (E * sdl.mH - dl[0].mH)
-            elif ctx.bulk:
-                sig = torch.linalg.inv(g)
-            else:
-                sig = E * tSL - tHL - torch.linalg.inv(g)
-            ins = [g] + th + [t for t in dl if t is not None]
-            grads = torch.autograd.grad(sig, ins, grad_outputs=gsig, allow_unused=True)
-            V = grads[0]
-            # adjoint of the fixed point: Lambda = V + P^H Lambda Q^H by doubling
-            tau = z * tSLL.detach() - tHLL.detach()
-            taup = z * tSLL.detach().mH - tHLL.detach().mH
-            A = (gs @ tau).mH
-            B = (taup @ gs).mH
-            lam = V
-            for _ in range(64):
-                lam = lam + A @ lam @ B
-                A = A @ A
-                B = B @ B
-                if float(A.abs().amax()) * float(B.abs().amax()) < 1e-32:
-                    break
-            fval = torch.linalg.inv(z * tSL - tHL - (z * tSLL - tHLL) @ gs.detach() @ (z * tSLL.mH - tHLL.mH))
-            gth = torch.autograd.grad(fval, th, grad_outputs=lam, allow_unused=True)
-        out = []
-        for i in range(4):
-            a_ = grads[1 + i]
-            b_ = gth[i]
-            if a_ is None and b_ is None:
-                out.append(None)
-            else:
-                out.append((a_ if a_ is not None else 0) + (b_ if b_ is not None else 0))
-        k = 5
-        gdl = []
-        for t in dl:
-            if t is None:
-                gdl.append(None)
-            else:
-                gdl.append(grads[k])
-                k += 1
-        return (None, None, None, None) + tuple(out) + tuple(gdl)
+        form = 0 if hDL is not None else (1 if ctx.bulk else 2)
+        E = energies.detach().cpu().numpy() + ctx.E_ref
+        dH, dH01, dS, dS01, dHDL, dSDL = lead_adjoint(hL.detach(), hLL.detach(), sL.detach(), sLL.detach(),
+                                                      None if hDL is None else hDL.detach(),
+                                                      None if sDL is None else sDL.detach(),
+                                                      E, ctx.eta, gs, gsig, form)
+        # a real parameter receives the real part (the backward of its promotion to complex)
+        cast = lambda g, t: None if g is None else (g if t.is_complex() else g.real).to(t.dtype)
+        return (None, None, None, None, cast(dH, hL), cast(dH01, hLL), cast(dS, sL), cast(dS01, sLL),
+                cast(dHDL, hDL), cast(dSDL, sDL))
 
 
 def lead_self_energy(hL: torch.Tensor, hLL: torch.Tensor, sL: torch.Tensor, sLL: torch.Tensor,

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 ROOT = os.path.dirname(PKG)
 OUT = os.path.join(PKG, "libnegf_b200.so")
-SOURCES = ["rgf.cu", "rgf_mx.cu", "rgf_noalloc.cu", "lopez_sancho.cu"]
+SOURCES = ["rgf.cu", "rgf_mx.cu", "rgf_noalloc.cu", "lopez_sancho.cu", "products.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-v"]
 

@@ -25,8 +25,7 @@
 // or the bulk form Sigma = (E S - H) - g_s^-1 when the lead has no H_DL.
 #include <cstdio>
 #include "../../include/negf_b200.h"
-#include "cta_lu.cuh"
-#include "cta_stream.cuh"
+#include "lead_forms.cuh"
 
 namespace negf {
 
@@ -39,59 +38,17 @@ __host__ __device__ inline size_t ls_slot_elems(const NegfLsProblem& p) {
   return (e + 15) & ~(size_t)15;
 }
 
-// out[i][j] = conj(X[j][i]) - z conj(Y[j][i])   (n x n), i.e. X^H - z Y^H
-NEGF_DEV void form_herm_shift(cplx* out, const cplx* X, const cplx* Y, cplx z, int n) {
-#pragma unroll 4
-  for (int e = threadIdx.x; e < n * n; e += CTA_THREADS) {
-    int i = e / n, j = e % n;
-    cplx x = cconj(X[(int64_t)j * n + i]), y = cconj(Y[(int64_t)j * n + i]);
-    out[e] = csub(x, cmul(z, y));
-  }
-  __syncthreads();
-}
-
-// out[i][j] = z conj(S[j][i]) - conj(H[j][i])   for an (rows x cols) H/S pair
-// stored (cols x rows): E S^H - H^H.
-NEGF_DEV void form_eS_minus_h_herm(cplx* out, const cplx* H, const cplx* S, cplx z, int rows, int cols) {
-  for (int e = threadIdx.x; e < rows * cols; e += CTA_THREADS) {
-    int i = e / cols, j = e % cols;
-    cplx h = cconj(H[(int64_t)j * rows + i]), s = cconj(S[(int64_t)j * rows + i]);
-    out[e] = csub(cmul(z, s), h);
-  }
-  __syncthreads();
-}
-
-NEGF_DEV double cta_max(double v, double* red) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
-  __syncthreads();
-  if (lane == 0) red[warp] = v;
-  __syncthreads();
-  double m = red[0];
-  for (int w = 1; w < CTA_THREADS / 32; ++w) m = fmax(m, red[w]);
-  __syncthreads();
-  return m;
-}
-
-template <int OPA, int OPB>
-NEGF_DEV void gemm_ls(cplx* smem, int M, int N, int K, const cplx* A, int64_t lda, const cplx* B, int64_t ldb,
-                      cplx* C, int64_t ldc, const cplx* D = nullptr, int64_t ldd = 0,
-                      cplx alpha = cmk(1.0, 0.0), cplx beta = cmk(1.0, 0.0)) {
-  GemmArgs g = gemm_args(M, N, K, A, lda, B, ldb, C, ldc);
-  g.alpha = alpha;
-  if (D) { g.D = D; g.ldd = ldd; g.beta = beta; g.use_d = true; }
-  // conventional 4M products (see warp_mma_3m); lead blocks come in every size, so warps
-  // outside the product skip their MMAs
-  cta_gemm<OPA, OPB, false, true>(g, smem);
-}
-
 NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, char* smem_raw, double* red) {
   cplx* smem = reinterpret_cast<cplx*>(smem_raw);
   const NegfLead ld = P.leads[it.lead];
   // every slot buffer holds max_n^2 elements: refuse a lead that would not fit (H_DL products are
-  // nc x b and nc x nc) before touching any memory
-  if (ld.n <= 0 || ld.n > P.max_n || ld.nc < 0 || ld.nc > P.max_n || (ld.nc > 0 && (ld.b <= 0 || ld.b > ld.n))) {
+  // nc x b and nc x nc) before touching any memory.  The coupling product alone reads g from the
+  // caller's memory and uses only nc x b and b x nc slot buffers.
+  const bool sig_only = it.mode == NEGF_LS_SIGMA_FROM_GS;
+  const bool bad_mode = it.mode != NEGF_LS_DECIMATE && !sig_only;
+  const bool bad_size = sig_only ? (ld.nc <= 0 || ld.nc > P.max_n || ld.b > P.max_n)
+                                 : (ld.n > P.max_n || ld.nc < 0 || ld.nc > P.max_n);
+  if (bad_mode || bad_size || ld.n <= 0 || (ld.nc > 0 && (ld.b <= 0 || ld.b > ld.n))) {
     if (threadIdx.x == 0) {
       P.status[it.out] = NEGF_ERR_ARGUMENT;
       if (P.iters) P.iters[it.out] = 0;
@@ -121,15 +78,35 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
   cplx *Ya = b_[8], *Yb = b_[9];  // separate n x n work blocks once the doubling is done
   const int n2c = 2 * n;
   int bad = 0;
-  // out = W^-1 (n x n) by the LU solve against I (numpy.linalg.inv's route); W is destroyed
-  auto lu_inverse = [&](cplx* W, cplx* out) {
-    int f = cta_lu_factor(W, n, n, smem_raw);
-    const int* perm = cta_lu_perm(smem_raw, n);
-    for (int e = threadIdx.x; e < n2; e += CTA_THREADS) out[e] = cmk(perm[e / n] == e % n ? 1.0 : 0.0, 0.0);
+  auto lu_inverse = [&](cplx* W, cplx* out) { return cta_lu_inverse(W, out, n, smem_raw); };
+  // Sigma = (E S_DL - H_DL) g[:b,:b] (E S_DL^H - H_DL^H) (selfEnergy, negf/surface_green.py:73-86)
+  auto coupling_sigma = [&](const cplx* g, cplx* sig) {
+    const int nc = ld.nc, b = ld.b;
+    const cplx* hdl = ar + ld.hdl;
+    const cplx* sdl = ar + ld.sdl;
+    // t1 = E S_DL - H_DL  (nc x b)
+    for (int e = threadIdx.x; e < nc * b; e += CTA_THREADS) t1[e] = csub(cmul(E, sdl[e]), hdl[e]);
     __syncthreads();
-    cta_lu_trsolve(W, n, n, out, n, n, smem_raw);
-    return f;
+    // t2 = E S_DL^H - H_DL^H (b x nc)
+    form_eS_minus_h_herm(t2, hdl, sdl, E, b, nc);
+    gemm_ls<OP_N, OP_N>(smem, nc, b, b, t1, b, g, n, Ya, b);   // (E S_DL - H_DL) g[:b,:b]
+    gemm_ls<OP_N, OP_N>(smem, nc, nc, b, Ya, b, t2, nc, sig, nc);
   };
+
+  if (sig_only) {
+    // the coupling product alone, on a surface Green's function the caller supplies (Bloch-unfolded
+    // leads build g from the decimations of the folded cell)
+    int st = NEGF_OK;
+    if (it.gs && it.sigma) coupling_sigma(reinterpret_cast<const cplx*>(it.gs), reinterpret_cast<cplx*>(it.sigma));
+    else st = NEGF_ERR_ARGUMENT;
+    if (threadIdx.x == 0) {
+      P.status[it.out] = st;
+      if (P.iters) P.iters[it.out] = 0;
+      if (P.resid) P.resid[it.out] = 0.0;
+    }
+    __syncthreads();
+    return;
+  }
 
   // alpha = h10 - z s10 = h01^H - z s01^H ; beta = h01 - z s01 ; eps = eps_s = H
   form_herm_shift(AB, h01, s01, z, n);
@@ -213,16 +190,7 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
     if (it.sigma && st != NEGF_ERR_LS_RESIDUAL) {
       cplx* sig = reinterpret_cast<cplx*>(it.sigma);
       if (ld.nc > 0) {
-        const int nc = ld.nc, b = ld.b;
-        const cplx* hdl = ar + ld.hdl;
-        const cplx* sdl = ar + ld.sdl;
-        // t1 = E S_DL - H_DL  (nc x b)
-        for (int e = threadIdx.x; e < nc * b; e += CTA_THREADS) t1[e] = csub(cmul(E, sdl[e]), hdl[e]);
-        __syncthreads();
-        // t2 = E S_DL^H - H_DL^H (b x nc)
-        form_eS_minus_h_herm(t2, hdl, sdl, E, b, nc);
-        gemm_ls<OP_N, OP_N>(smem, nc, b, b, t1, b, gs, n, Ya, b);   // (E S_DL - H_DL) g_s[:b,:b]
-        gemm_ls<OP_N, OP_N>(smem, nc, nc, b, Ya, b, t2, nc, sig, nc);
+        coupling_sigma(gs, sig);
       } else {
         // bulk form: Sigma = (E S - H) - g_s^-1
         cta_shift_form(A, gs, nullptr, cmk(0.0, 0.0), ONE, (int)n2, smem);
@@ -260,11 +228,7 @@ __global__ void __launch_bounds__(CTA_THREADS, 1) ls_kernel(const NegfLsProblem 
   }
 }
 
-size_t ls_smem_bytes(int max_n) {
-  size_t a = GEMM_SMEM_BYTES, b = lu_smem_bytes_host(max_n), c = STREAM_SMEM_BYTES;
-  size_t m = a > b ? a : b;
-  return m > c ? m : c;
-}
+size_t ls_smem_bytes(int max_n) { return lead_smem_bytes(max_n); }
 
 }  // namespace negf
 

@@ -78,6 +78,9 @@ size_t negf_abi_struct_size(int which) {
     case 4: return sizeof(NegfLead);
     case 5: return sizeof(NegfLsItem);
     case 6: return sizeof(NegfLsProblem);
+    case 7: return sizeof(NegfGammaSum);
+    case 8: return sizeof(NegfLeadAdjItem);
+    case 9: return sizeof(NegfLeadAdjProblem);
     default: return 0;
   }
 }

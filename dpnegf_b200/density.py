@@ -27,6 +27,7 @@ import numpy as np
 import torch
 
 from .negf_utils import gauss_xw
+from .products import gamma_sum
 from .ozaki_res_cal import ozaki_residues
 
 log = logging.getLogger(__name__)
@@ -88,15 +89,17 @@ class Ozaki(Density):
             Gr = self._green_first_block(deviceprop, kpoint, xs.to(torch.complex128), eta_lead, eta_device,
                                          None, block_tridiagonal)
             gam = deviceprop.lead_R.gamma.to(Gr.device)
+            if gam.ndim == 2:
+                gam = gam.unsqueeze(0)
             n0 = Gr.shape[-1]
             cr = min(n0, gam.shape[-1])
-            GR = torch.zeros(gam.shape[0], n0, n0, dtype=torch.complex128, device=Gr.device)
-            GR[:, n0 - cr:, n0 - cr:] = gam[:, gam.shape[-2] - cr:, gam.shape[-1] - cr:]
-            A = (Gr @ GR @ Gr.mH).real
             # f_R - f_L per node on 0-d host tensors, the reference's arithmetic (density.py:192)
             df = torch.stack([torch.as_tensor(deviceprop.lead_R.fermi_dirac(x + mu_D)
                                               - deviceprop.lead_L.fermi_dirac(x + mu_D)).real.cpu() for x in xs])
-            DM_neq = (wlg.to(Gr.device).reshape(-1, 1, 1) * (A * df.to(Gr.device).reshape(-1, 1, 1))).sum(0)
+            # sum_i wlg_i df_i Re(G_i Gamma_R G_i^H) with Gamma_R in the last cr x cr corner: one CUDA
+            # call (per-node products, then one GEMM over every node)
+            w = wlg.to(torch.float64) * df.to(torch.float64)
+            DM_neq = gamma_sum(Gr, gam[:, gam.shape[-2] - cr:, gam.shape[-1] - cr:], n0 - cr, w)
         else:
             DM_neq = 0.
         return DM_eq, DM_neq

@@ -25,6 +25,7 @@ from scipy.constants import Boltzmann
 
 from .bloch import Bloch
 from .surface_green import LeadArena, LeadBlocks, self_energies
+from .products import coupling_sigma
 
 log = logging.getLogger(__name__)
 eV2J = 1.6021766208e-19  # J per eV, as in dpnegf/utils/constants.py
@@ -173,18 +174,18 @@ class LeadProperty(object):
                     if i != j:
                         ph[i, j] = torch.exp(1j * 2 * torch.pi * torch.dot(R[j] - R[i], kbt))
             g = torch.stack(res.gs[ik * nE:(ik + 1) * nE])  # [nE, n, n]
-            term = torch.stack([torch.kron(ph.to(dev), g[e]) for e in range(nE)])
+            n1 = g.shape[-1]
+            # kron(ph, g[e]) for every energy at once: [e, i n1 + a, j n1 + c] = ph[i, j] g[e, a, c]
+            term = (ph.to(dev).view(1, m_size, 1, m_size, 1) * g.view(nE, 1, n1, 1, n1)).reshape(
+                nE, m_size * n1, m_size * n1)
             sgf = term if sgf is None else sgf + term
         sgf = sgf / nk
         idxs = torch.as_tensor(self.bloch_sorted_indice, device=dev)
         sgf = sgf[:, idxs, :][:, :, idxs]
         hdl, sdl = self.HDL_reduced(torch.as_tensor(self.HDLk), torch.as_tensor(self.SDLk), subblocks)
-        hdl, sdl = hdl.to(dev, torch.complex128), sdl.to(dev, torch.complex128)
-        b = torch.as_tensor(self.HDLk).shape[1]
-        Es = torch.as_tensor(E, device=dev).reshape(-1, 1, 1) + complex(self.E_ref)
-        left = Es * sdl - hdl
-        right = Es * sdl.conj().T - hdl.conj().T
-        return left @ sgf[:, :b, :b] @ right
+        # (E S_DL - H_DL) sgf[:b,:b] (E S_DL^H - H_DL^H) for every energy: the decimation kernel's
+        # coupling product on the unfolded surface Green's functions (one launch)
+        return coupling_sigma(sgf, hdl, sdl, E, E_ref=self.E_ref)
 
     @staticmethod
     def HDL_reduced(HDL: torch.Tensor, SDL: torch.Tensor, subblocks) -> torch.Tensor:

@@ -187,9 +187,16 @@ typedef struct NegfLead {
 } NegfLead;
 
 /* One decimation: a lead at one energy. */
+/* NegfLsItem.mode */
+#define NEGF_LS_DECIMATE 0       /* decimation, g_s, residual check, Sigma */
+#define NEGF_LS_SIGMA_FROM_GS 1  /* Sigma = (E S_DL - H_DL) g[:b,:b] (E S_DL^H - H_DL^H) from the item's gs as INPUT
+                                    (lead.n x lead.n, row stride lead.n) with no decimation; needs lead.nc > 0.
+                                    The Bloch-unfolded self-energy of LeadProperty.self_energy
+                                    (negf/lead_property.py:330-379) builds g from the folded cell's decimations */
+
 typedef struct NegfLsItem {
   int32_t lead;
-  int32_t pad;
+  int32_t mode;      /* NEGF_LS_DECIMATE or NEGF_LS_SIGMA_FROM_GS */
   double e_re, e_im; /* E = energy + E_ref (may be complex, e.g. Ozaki poles) */
   double eta;        /* decimation runs at z = E + i eta (surface_green.py:65-70, :83) */
   double* sigma;     /* complex128 [nc x nc] (or [n x n] bulk form) output; NULL = not wanted */
@@ -226,6 +233,68 @@ size_t negf_lopez_sancho_scratch_bytes(const NegfLsProblem* p);
  * until max(|alpha| + |beta|) < tol; g_s = (zS - eps_s)^-1 with the residual
  * check of :142-155; Sigma = (E S_DL - H_DL) g_s[:b,:b] (E S_DL^H - H_DL^H). */
 int negf_lopez_sancho_run(const NegfLsProblem* p, void* cuda_stream);
+
+/* Weighted sum of G Gamma G^H products over energies:
+ *   out = sum_i w_i Re(G_i[:, c0:c0+k] Gamma_i G_i[:, c0:c0+k]^H)      (real n x n, row stride n)
+ * the non-equilibrium density matrix of Ozaki.integrate (negf/density.py:183-195:
+ * DM_neq = sum_i wlg_i (G_i Gamma_R,i G_i^H).real (f_R - f_L)(x_i), Gamma_R in the corner of G). */
+typedef struct NegfGammaSum {
+  const double* g;       /* complex128; item i's G at g + i * g_stride (complex elements), n rows of stride ldg */
+  int64_t g_stride;
+  const double* gamma;   /* complex128; item i's Gamma (k x k, row stride ldgam) at gamma + i * gamma_stride */
+  int64_t gamma_stride;
+  const double* w;       /* [n_items] real weights (device memory) */
+  double* out;           /* [n x n] real output (device memory) */
+  int32_t n_items;
+  int32_t n;             /* rows of G and of out */
+  int32_t ldg;           /* >= c0 + k */
+  int32_t c0;            /* first column of G that Gamma couples to */
+  int32_t k;             /* size of Gamma */
+  int32_t ldgam;         /* >= k */
+  void* scratch;         /* 256-byte aligned, negf_gamma_sum_scratch_bytes */
+  size_t scratch_bytes;
+} NegfGammaSum;
+
+size_t negf_gamma_sum_scratch_bytes(const NegfGammaSum* p);
+/* Two launches on the stream: per-energy products, then one GEMM over all energies in order
+ * (bitwise reproducible).  Returns NEGF_OK or a call-level error. */
+int negf_gamma_sum_run(const NegfGammaSum* p, void* cuda_stream);
+
+/* Gradient of a loss through one lead's self-energies at many energies, by implicit
+ * differentiation of the converged decimation: g_s is the fixed point of
+ * f(g) = (zS - H - tau g tau')^-1, tau = z S01 - H01, tau' = z S01^H - H01^H (the relation
+ * the reference's residual check tests, negf/surface_green.py:142-145).  With V = dL/dg_s from
+ * Sigma(g_s), Lambda = V + (g_s tau)^H Lambda (tau' g_s)^H is solved by doubling and
+ * dL/dtheta = Lambda-weighted derivative of f at the fixed point, plus Sigma's explicit terms.
+ * No reference counterpart: the reference differentiates through its decimation loop with
+ * torch autograd. */
+typedef struct NegfLeadAdjItem {
+  double e_re, e_im;     /* E = energy + E_ref (Sigma uses E; g_s was computed at z = E + i eta) */
+  const double* gs;      /* complex128 [n x n] converged g_s */
+  const double* gsig;    /* complex128 dL/dSigma (PyTorch convention): [nc x nc] for form 0, else [n x n] */
+} NegfLeadAdjItem;
+
+typedef struct NegfLeadAdjProblem {
+  NegfLead lead;                /* blocks as offsets into arena; hdl/sdl used by form 0 */
+  const double* arena;          /* complex128 lead blocks */
+  const NegfLeadAdjItem* items; /* device memory */
+  int32_t n_items;
+  int32_t form;                 /* 0: Sigma = (E S_DL - H_DL) g_s[:b,:b] (E S_DL^H - H_DL^H);
+                                   1: Sigma = g_s^-1; 2: Sigma = E S - H - g_s^-1 */
+  double eta;
+  double tol;                   /* doubling stops once max|P| max|Q| < tol */
+  int32_t max_iter;             /* doubling steps at most */
+  int32_t n_slots;              /* CTAs; energies go to them round-robin */
+  double* grad;                 /* complex128 out: dL/dH, dL/dH01, dL/dS, dL/dS01 [n x n] each, then
+                                   dL/dH_DL, dL/dS_DL [nc x b] each for form 0; summed over energies */
+  int32_t* status;              /* [n_items] NEGF_OK, NEGF_ERR_SINGULAR, NEGF_ERR_NONFINITE */
+  int32_t* iters;               /* [n_items] doubling steps (may be NULL) */
+  void* scratch;                /* 256-byte aligned, negf_lead_adjoint_scratch_bytes */
+  size_t scratch_bytes;
+} NegfLeadAdjProblem;
+
+size_t negf_lead_adjoint_scratch_bytes(const NegfLeadAdjProblem* p);
+int negf_lead_adjoint_run(const NegfLeadAdjProblem* p, void* cuda_stream);
 
 /* Bytes of scratch negf_rgf_run needs for p->n_slots, p->max_n, p->max_g_slab, p->flags. */
 size_t negf_rgf_scratch_bytes(const NegfRgfProblem* p);
@@ -270,7 +339,8 @@ int negf_sm_count(void);
 const char* negf_version(void);
 
 /* sizeof of the ABI structs (0 NegfBlock, 1 NegfDevice, 2 NegfItem,
- * 3 NegfRgfProblem, 4 NegfLead, 5 NegfLsItem, 6 NegfLsProblem) so bindings
+ * 3 NegfRgfProblem, 4 NegfLead, 5 NegfLsItem, 6 NegfLsProblem, 7 NegfGammaSum,
+ * 8 NegfLeadAdjItem, 9 NegfLeadAdjProblem) so bindings
  * can verify their mirrors; 0 if unknown. */
 size_t negf_abi_struct_size(int which);
 

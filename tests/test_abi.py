@@ -46,6 +46,10 @@ def test_struct_mirrors_match_c_sizes():
     assert lib.negf_abi_struct_size(4) == _lib.LEAD_DTYPE.itemsize
     assert lib.negf_abi_struct_size(5) == _lib.LS_ITEM_DTYPE.itemsize
     assert lib.negf_abi_struct_size(6) == ctypes.sizeof(_lib.NegfLsProblem)
+    assert lib.negf_abi_struct_size(7) == ctypes.sizeof(_lib.NegfGammaSum)
+    assert lib.negf_abi_struct_size(8) == _lib.LEADADJ_ITEM_DTYPE.itemsize
+    assert lib.negf_abi_struct_size(9) == ctypes.sizeof(_lib.NegfLeadAdjProblem)
+    assert ctypes.sizeof(_lib.NegfLead) == _lib.LEAD_DTYPE.itemsize
 
 
 def test_scratch_query_without_gpu():

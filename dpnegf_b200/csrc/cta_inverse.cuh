@@ -99,6 +99,26 @@ NEGF_DEV double pivot_measure(cplx a) {
   return (v == v) ? v : INFINITY;  // NaN pivots are taken (and flagged) first
 }
 
+// The same search on integer keys: a pivot measure is >= 0 or +inf, and for such doubles the
+// order of the IEEE bit patterns read as signed 64-bit integers is the numeric order, so the
+// winner (ties to the lower index) is the one the double comparison picks, while the compares
+// and shuffles stay on the integer pipes instead of the long-latency FP64 ones.  -1 is "no
+// candidate"; a key <= 0 (zero pivot) or >= PIVOT_KEY_INF (infinite or NaN) is singular.
+constexpr long long PIVOT_KEY_INF = 0x7ff0000000000000LL;
+NEGF_DEV long long pivot_key(cplx a) { return __double_as_longlong(pivot_measure(a)); }
+NEGF_DEV void argmax_merge_key(long long& v, int& i, long long ov, int oi) {
+  if (ov > v || (ov == v && oi < i)) { v = ov; i = oi; }
+}
+NEGF_DEV void warp_argmax_key(long long& v, int& i) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const long long ov = __shfl_xor_sync(0xffffffffu, v, off);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, off);
+    argmax_merge_key(v, i, ov, oi);
+  }
+}
+NEGF_DEV bool pivot_key_singular(long long k) { return k <= 0 || k >= PIVOT_KEY_INF; }
+
 // Outer-update epilogue: pivot rows of the block take the product, the other
 // rows add it to their current value.
 struct EpiGJ {
@@ -123,7 +143,7 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
   constexpr int PP = InvLayout<NB>::PP;
   constexpr int RP = InvLayout<NB>::RP;
   constexpr int NWARP = CTA_THREADS / 32;
-  static_assert(NB * RT == 32, "a thread holds RT panel rows of NB complex entries");
+  static_assert(NB * RT <= 32, "a thread holds RT panel rows of NB complex entries (n <= 256 RT)");
   const int n_pad = InvLayout<NB>::rows(n);
   cplx* P = reinterpret_cast<cplx*>(smem_raw);
   cplx* Rb[2] = {P + (size_t)n_pad * PP, P + (size_t)n_pad * PP + NB * RP};
@@ -132,7 +152,7 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
   int* pinv = piv + n;                           // physical row -> logical column (-1: unused)
   int* red_i = pinv + n;                         // [2][NWARP] pivot candidates (double buffered)
   int* s_misc = red_i + 2 * NWARP;               // [1]: singular flag
-  double* red_v = reinterpret_cast<double*>(s_misc + 48);  // [2][NWARP]
+  long long* red_v = reinterpret_cast<long long*>(s_misc + 48);  // [2][NWARP] pivot keys
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = (warp >> 2) * 32, wn = (warp & 3) * 16;
   // Panel rows owned by this thread: tid + 256 r, r < RT (n <= 256 RT).
@@ -146,17 +166,17 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
 
   // Every thread merges the per-warp candidates (one barrier per pivot) and
   // marks the winner as used; thread 0 records it for the updates and gather.
-  auto choose_pivot = [&](double v, int i, int c) -> int {
-    warp_argmax(v, i);
+  auto choose_pivot = [&](long long v, int i, int c) -> int {
+    warp_argmax_key(v, i);
     if (lane == 0) { red_v[par * NWARP + warp] = v; red_i[par * NWARP + warp] = i; }
     __syncthreads();
-    double bv = red_v[par * NWARP];
+    long long bv = red_v[par * NWARP];
     int bi = red_i[par * NWARP];
 #pragma unroll
-    for (int k = 1; k < NWARP; ++k) argmax_merge(bv, bi, red_v[par * NWARP + k], red_i[par * NWARP + k]);
+    for (int k = 1; k < NWARP; ++k) argmax_merge_key(bv, bi, red_v[par * NWARP + k], red_i[par * NWARP + k]);
     par ^= 1;
     if (tid == 0) {
-      if (!(bv > 0.0) || !isfinite(bv)) s_misc[1] = 1;
+      if (pivot_key_singular(bv)) s_misc[1] = 1;
       piv[c] = bi;
       pinv[bi] = c;
     }
@@ -181,7 +201,7 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
       // each thread takes its rows (tid + 256 r) of the panel into registers
       cplx row[RT][NB];
       cplx mm[RT];  // the rows' entries in the column being eliminated
-      double bv = -1.0;
+      long long bv = -1;
       int bi = n;
 #pragma unroll
       for (int r = 0; r < RT; ++r) {
@@ -189,7 +209,7 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
 #pragma unroll
         for (int k = 0; k < NB; ++k) row[r][k] = (i < n) ? P[i * PP + k] : cmk(0.0, 0.0);
         mm[r] = row[r][0];
-        if (i < n && !((used >> r) & 1u)) argmax_merge(bv, bi, pivot_measure(mm[r]), i);
+        if (i < n && !((used >> r) & 1u)) argmax_merge_key(bv, bi, pivot_key(mm[r]), i);
       }
       int p = choose_pivot(bv, bi, p0);
       pc->mark(PH_INV_STAGE);
@@ -214,7 +234,7 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
         }
         __syncthreads();
         const int nxt = jj + 1;
-        bv = -1.0;
+        bv = -1;
         bi = n;
 #pragma unroll
         for (int r = 0; r < RT; ++r) {
@@ -236,7 +256,7 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
               for (int k = 0; k < NB; ++k)
                 if (k == nxt) mnext = row[r][k];
             }
-            if (nxt < w && i != p && !((used >> r) & 1u)) argmax_merge(bv, bi, pivot_measure(mnext), i);
+            if (nxt < w && i != p && !((used >> r) & 1u)) argmax_merge_key(bv, bi, pivot_key(mnext), i);
           }
           mm[r] = mnext;
         }
@@ -367,8 +387,9 @@ NEGF_DEV int cta_inverse(cplx* W, int64_t ldw, int n, cplx* G, int64_t ldg, char
                          cplx* snap, int ob = INV_OB) {
   // 16-wide panels for small blocks (the block inverse's 64-wide leaves): a column step's
   // latency chain is shorter, measured 22 % faster at n = 64 (8 % at n = 128, where the
-  // rank-16 updates start to cost more)
+  // rank-16 updates start to cost more).  One register row per thread up to n = 256.
   if (n > 64 && n <= 256) return cta_inverse_nb<32, 1, G3, TC>(W, ldw, n, G, ldg, smem_raw, pc, snap, ob);
+  if (n <= 64) return cta_inverse_nb<16, 1, G3, TC>(W, ldw, n, G, ldg, smem_raw, pc, snap, ob);
   return cta_inverse_nb<16, 2, G3, TC>(W, ldw, n, G, ldg, smem_raw, pc, snap, ob);
 }
 

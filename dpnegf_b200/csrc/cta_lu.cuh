@@ -66,7 +66,7 @@ struct LuCtx {
   int n;
   char* smem;
   cplx* rdiag;    // [LU_TB] reciprocal diagonal of the current upper block
-  double* red_v;  // [8] pivot candidates
+  long long* red_v;  // [8] pivot candidates (keys, see pivot_key)
   int* red_i;     // [8]
   int* flag;      // [1] zero / non-finite pivot met
   int* ipiv;      // [n] row swapped with row k at step k (LAPACK order)
@@ -119,16 +119,16 @@ NEGF_DEV void lu_panel(const LuCtx& c, int r0, int w) {
   }
   __syncthreads();
   for (int j = 0; j < w; ++j) {
-    double bv = -1.0;
+    long long bv = -1;
     int bi = m;
-    for (int r = j + tid; r < m; r += CTA_THREADS) argmax_merge(bv, bi, pivot_measure(P[r * PP + j]), r);
-    warp_argmax(bv, bi);
+    for (int r = j + tid; r < m; r += CTA_THREADS) argmax_merge_key(bv, bi, pivot_key(P[r * PP + j]), r);
+    warp_argmax_key(bv, bi);
     if (lane == 0) { c.red_v[warp] = bv; c.red_i[warp] = bi; }
     __syncthreads();
     bv = c.red_v[0];
     bi = c.red_i[0];
 #pragma unroll
-    for (int k = 1; k < NWARP; ++k) argmax_merge(bv, bi, c.red_v[k], c.red_i[k]);
+    for (int k = 1; k < NWARP; ++k) argmax_merge_key(bv, bi, c.red_v[k], c.red_i[k]);
     if (bi != j)
       for (int k = tid; k < NB; k += CTA_THREADS) {
         const cplx t = P[j * PP + k];
@@ -137,7 +137,7 @@ NEGF_DEV void lu_panel(const LuCtx& c, int r0, int w) {
       }
     if (tid == 0) {
       c.ipiv[r0 + j] = r0 + bi;
-      if (!(bv > 0.0) || !isfinite(bv)) *c.flag = 1;
+      if (pivot_key_singular(bv)) *c.flag = 1;
     }
     __syncthreads();
     const cplx d = crcp_fast(P[j * PP + j]);
@@ -275,7 +275,7 @@ NEGF_DEV LuCtx lu_ctx(cplx* W, int64_t ldw, int n, char* smem_raw, PhaseClock* p
   LuCtx c;
   c.W = W; c.ldw = ldw; c.n = n; c.smem = smem_raw;
   c.rdiag = reinterpret_cast<cplx*>(sm);
-  c.red_v = reinterpret_cast<double*>(c.rdiag + LU_TB);
+  c.red_v = reinterpret_cast<long long*>(c.rdiag + LU_TB);
   c.red_i = reinterpret_cast<int*>(c.red_v + 8);
   c.flag = c.red_i + 8;
   c.ipiv = c.flag + 4;

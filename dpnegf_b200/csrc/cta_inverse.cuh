@@ -32,6 +32,14 @@
 
 namespace negf {
 
+#ifndef NEGF_INV_SMALL_NB
+#define NEGF_INV_SMALL_NB 8
+#endif
+// Panel width of the Gauss-Jordan inverse for blocks of n <= 64 (the block inverse's leaves).
+// Measured against 16-wide panels (every SM inverting its own matrices): 4-9 % faster for
+// n = 32..64, 2-3 % for the block inverse of n = 128..192, equal at n = 256 and n = 16.
+constexpr int INV_SMALL_NB = NEGF_INV_SMALL_NB;
+static_assert(INV_SMALL_NB == 8 || INV_SMALL_NB == 16, "8- or 16-wide panels for small blocks");
 constexpr int INV_OB = 128;      // default outer block (columns) of the two-level Gauss-Jordan
 constexpr int INV_OB_MAX = 512;  // widest outer block (one block: no outer update for n <= 512)
 
@@ -61,7 +69,7 @@ struct InvLayout {
 // 32-wide panels, the others 16-wide panels, and a device may mix both.
 inline size_t inv_smem_bytes_host(int max_n, bool tc = false) {
   size_t a = InvLayout<32>::bytes(max_n < 256 ? max_n : 256, tc);
-  const size_t s = InvLayout<16>::bytes(max_n < 64 ? max_n : 64, tc);
+  const size_t s = InvLayout<INV_SMALL_NB>::bytes(max_n < 64 ? max_n : 64, tc);
   if (s > a) a = s;
   if (max_n > 256) {
     const size_t b = InvLayout<16>::bytes(max_n, tc);
@@ -385,11 +393,12 @@ __device__ __noinline__ int cta_inverse_nb(cplx* W, int64_t ldw, int n, cplx* G,
 template <bool G3 = true, bool TC = false>
 NEGF_DEV int cta_inverse(cplx* W, int64_t ldw, int n, cplx* G, int64_t ldg, char* smem_raw, PhaseClock* pc,
                          cplx* snap, int ob = INV_OB) {
-  // 16-wide panels for small blocks (the block inverse's 64-wide leaves): a column step's
-  // latency chain is shorter, measured 22 % faster at n = 64 (8 % at n = 128, where the
-  // rank-16 updates start to cost more).  One register row per thread up to n = 256.
+  // Narrow panels for small blocks (the block inverse's 64-wide leaves): a column step's
+  // latency chain is shorter (16-wide measured 22 % faster than 32-wide at n = 64, 8 % at
+  // n = 128, where the rank-16 updates start to cost more; 8-wide another 4-9 % for n <= 64).
+  // One register row per thread up to n = 256.
   if (n > 64 && n <= 256) return cta_inverse_nb<32, 1, G3, TC>(W, ldw, n, G, ldg, smem_raw, pc, snap, ob);
-  if (n <= 64) return cta_inverse_nb<16, 1, G3, TC>(W, ldw, n, G, ldg, smem_raw, pc, snap, ob);
+  if (n <= 64) return cta_inverse_nb<INV_SMALL_NB, 1, G3, TC>(W, ldw, n, G, ldg, smem_raw, pc, snap, ob);
   return cta_inverse_nb<16, 2, G3, TC>(W, ldw, n, G, ldg, smem_raw, pc, snap, ob);
 }
 

@@ -55,8 +55,9 @@ def parse():
     ap.add_argument("--refine-steps", type=int, default=3)
     ap.add_argument("--configs", default="",
                     help="extra legs, comma separated: 'uneven' (the 512-device uneven batch, 128 devices), "
-                         "'leads' (its lead decimation alone, --lead-devices devices) and 'scf' (b=512 SCF "
-                         "loop captured as a CUDA graph); not in the default run")
+                         "'leads' (its lead decimation alone, --lead-devices devices), 'scf' (b=512 SCF "
+                         "loop captured as a CUDA graph) and 'products' (the G Gamma G^H sum, the Bloch "
+                         "coupling product and the lead adjoint, each timed alone); not in the default run")
     ap.add_argument("--lead-devices", type=int, default=128, help="devices whose leads the 'leads' leg decimates")
     ap.add_argument("--lead-eta", type=float, default=1e-5, help="lead broadening of the 'leads' leg")
     ap.add_argument("--no-leads", action="store_true", help="skip the metric device's lead decimation object")
@@ -332,6 +333,61 @@ def _timed(torch, fn):
 # Lead broadening of the synthetic leads (edge blocks of random dense devices) in the opt-in legs;
 # the decimation's LU solve keeps the residual check within the reference's bound at 1e-5.
 ETA_LEAD_SYNTH = 1e-5
+
+
+def products_leg(torch, peak, n=256, n_nodes=256, n_bloch=256, n_lead_e=64, eta=ETA_LEAD_SYNTH, seed=77):
+    """The product chains beside the sweep, each timed alone through its Python API with CUDA
+    events (descriptor packing and the status read included): the DM_neq sum of Ozaki.integrate
+    (negf_gamma_sum_run) over n_nodes Gauss nodes of an n x n first block with an n x n Gamma_R;
+    the Bloch coupling product (the decimation kernel's coupling mode) on n_bloch unfolded
+    2n x 2n surface Green's functions with an n x n H_DL; the lead-parameter adjoint
+    (negf_lead_adjoint_run) of the b = n metric device's left lead at n_lead_e energies.  Work is
+    counted as 8 flop per complex multiply-add (4M), as for the sweep."""
+    from dpnegf_b200 import products, workload
+    from dpnegf_b200.surface_green import LeadArena, LeadBlocks, self_energies
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    rnd = lambda *s: torch.randn(*s, dtype=torch.complex128, device="cuda", generator=gen) / n ** 0.5
+    res = {}
+
+    def rec(name, ms, flop, shape):
+        tf = flop / ms / 1e9
+        res[name] = {"ms": ms, "tflops_algorithmic": tf, "frac_of_dgemm": tf / peak, "shape": shape}
+
+    G, gam = rnd(n_nodes, n, n), rnd(n_nodes, n, n)
+    w = torch.rand(n_nodes, dtype=torch.float64)
+    products.gamma_sum(G, gam, 0, w)
+    _, ms = _timed(torch, lambda: products.gamma_sum(G, gam, 0, w))
+    rec("gamma_sum", ms, 8.0 * 2 * n_nodes * n ** 3, f"{n_nodes} nodes, G {n}x{n}, Gamma {n}x{n}")
+    del G, gam
+
+    g = rnd(n_bloch, 2 * n, 2 * n)
+    hdl, sdl = rnd(n, n), rnd(n, n) * 0.05
+    E = np.linspace(-1.0, 1.0, n_bloch)
+    products.coupling_sigma(g, hdl, sdl, E)
+    _, ms = _timed(torch, lambda: products.coupling_sigma(g, hdl, sdl, E))
+    rec("bloch_coupling", ms, 8.0 * 2 * n_bloch * n ** 3, f"{n_bloch} energies, g {2 * n}x{2 * n}, H_DL {n}x{n}")
+    del g
+
+    ld = workload.random_device(n, 2, seed=seed).lead_L
+    lead = LeadBlocks(ld.hL, ld.hLL, ld.sL, ld.sLL, ld.hDL, ld.sDL)
+    El = np.linspace(-2.5, 2.5, n_lead_e)
+    dec = self_energies(LeadArena([lead]), [0] * n_lead_e, El, eta, want_gs=True, check=False)
+    gs = torch.stack(dec.gs)
+    nc = ld.hDL.shape[0]
+    gsig = rnd(n_lead_e, nc, nc)
+    info = {}
+    args = (ld.hL, ld.hLL, ld.sL, ld.sLL, ld.hDL, ld.sDL, El, eta, gs, gsig, 0)
+    products.lead_adjoint(*args)
+    _, ms = _timed(torch, lambda: products.lead_adjoint(*args, info=info))
+    steps = info["iters"].astype(np.float64)
+    # per energy: V and the explicit H_DL/S_DL terms (5 products), 4 products per doubling step, then
+    # g tau', tau g tau', F^H Lambda, dW, dtau, tau g, dtau' (7 products) and one LU inverse (4/3 n^3)
+    flop = 8.0 * n ** 3 * float(np.sum(5.0 + 7.0 + 4.0 / 3.0 + 4.0 * steps))
+    rec("lead_adjoint", ms, flop, f"{n_lead_e} energies, lead {n}x{n}, H_DL {nc}x{ld.hDL.shape[1]}")
+    res["lead_adjoint"]["doubling_steps_mean"] = float(steps.mean())
+    res["note"] = ("each call timed once after a warm-up call, CUDA events around the Python API call; "
+                   "work at 8 flop per complex multiply-add; frac against the in-run DGEMM")
+    return res
 
 
 def _ls_flops(n, iters):
@@ -855,6 +911,8 @@ def main():
         if "scf" in wanted:
             extra["config5_scf"] = scf_leg(torch, peak, nk=args.scf_k, n_energies=args.scf_energies,
                                            iters=args.scf_iters, eta_lead=args.lead_eta)
+        if "products" in wanted:
+            extra["product_chains"] = products_leg(torch, peak, eta=args.lead_eta)
 
     # end-to-end through the public API: pinned host inputs, host outputs
     e2e = None

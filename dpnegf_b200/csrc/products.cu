@@ -19,16 +19,27 @@ namespace negf {
 // ---------------------------------------------------------------------------------------------
 // Weighted G Gamma G^H sum.  Stage 1 (one CTA per energy): T_i = w_i G_i[:, c0:] Gamma_i and a
 // copy of G_i[:, c0:], side by side as the column blocks of two n x (n_items k) matrices.
-// Stage 2 (one CTA per 64 x 64 output tile): out = Re(T_stack G_stack^H), one GEMM whose k-loop
-// runs over every energy in order.
+// Stage 2: out = Re(T_stack G_stack^H), one GEMM over every energy.  Its k-loop is split into
+// up to GS_MAX_SPLIT contiguous ranges so that the output tiles times the splits fill the GPU
+// (a 256 x 256 output is only 16 tiles); each (tile, range) CTA writes the real part of its
+// partial product, and stage 3 sums the ranges in range order, so the result does not depend
+// on scheduling.
 
 constexpr size_t PROD_ALIGN = 256;
+constexpr int GS_MAX_SPLIT = 16;
 
 inline size_t round_up(size_t b) { return (b + PROD_ALIGN - 1) & ~(PROD_ALIGN - 1); }
 
 inline size_t gamma_stack_bytes(const NegfGammaSum& p) {
   return round_up((size_t)p.n * (size_t)p.n_items * (size_t)p.k * sizeof(cplx));
 }
+
+inline size_t gamma_part_bytes(const NegfGammaSum& p) {
+  return round_up((size_t)GS_MAX_SPLIT * p.n * p.n * sizeof(double));
+}
+
+// k-range length of stage 2 for `split` ranges: a multiple of the 16-deep k slab.
+inline int64_t gamma_split_len(int64_t K, int split) { return ((K + split - 1) / split + 15) / 16 * 16; }
 
 __global__ void __launch_bounds__(CTA_THREADS, 1) gamma_stack_kernel(const NegfGammaSum P, cplx* Tst, cplx* Gst) {
   extern __shared__ __align__(16) char smem_raw[];
@@ -54,15 +65,33 @@ struct EpiRealOut {
   NEGF_DEV void operator()(int m, int n, cplx v) const { out[(int64_t)(m0 + m) * ld + n0 + n] = v.x; }
 };
 
+// Stage 2: CTA (x, y, z) multiplies output tile (y, x) over k-range z into part[z].
 __global__ void __launch_bounds__(CTA_THREADS, 1) gamma_reduce_kernel(const NegfGammaSum P, const cplx* Tst,
-                                                                      const cplx* Gst) {
+                                                                      const cplx* Gst, double* part,
+                                                                      int64_t klen) {
   extern __shared__ __align__(16) char smem_raw[];
   cplx* smem = reinterpret_cast<cplx*>(smem_raw);
   const int64_t K = (int64_t)P.n_items * P.k;
   const int m0 = blockIdx.y * GT_M, n0 = blockIdx.x * GT_N;
+  const int64_t k0 = (int64_t)blockIdx.z * klen;
   const int M = min(GT_M, P.n - m0), N = min(GT_N, P.n - n0);
-  GemmArgs g = gemm_args(M, N, (int)K, Tst + (int64_t)m0 * K, K, Gst + (int64_t)n0 * K, K, nullptr, 0);
-  cta_gemm_epi<OP_N, OP_C, false, EpiRealOut, true>(g, smem, EpiRealOut{P.out, P.n, m0, n0});
+  const int Kz = (int)(k0 < K ? (K - k0 < klen ? K - k0 : klen) : 0);
+  double* out = part + (size_t)blockIdx.z * P.n * P.n;
+  if (Kz == 0) {  // an empty range still writes its (zero) partial tile
+    for (int e = threadIdx.x; e < M * N; e += CTA_THREADS) out[(int64_t)(m0 + e / N) * P.n + n0 + e % N] = 0.0;
+    return;
+  }
+  GemmArgs g = gemm_args(M, N, Kz, Tst + (int64_t)m0 * K + k0, K, Gst + (int64_t)n0 * K + k0, K, nullptr, 0);
+  cta_gemm_epi<OP_N, OP_C, false, EpiRealOut, true>(g, smem, EpiRealOut{out, P.n, m0, n0});
+}
+
+// Stage 3: out = sum of the partial outputs in range order.
+__global__ void gamma_sum_parts_kernel(double* out, const double* part, int64_t n2, int split) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n2; e += (int64_t)gridDim.x * blockDim.x) {
+    double s = part[e];
+    for (int z = 1; z < split; ++z) s += part[(size_t)z * n2 + e];
+    out[e] = s;
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -251,7 +280,7 @@ extern "C" {
 
 size_t negf_gamma_sum_scratch_bytes(const NegfGammaSum* p) {
   if (!p || p->n <= 0 || p->k <= 0 || p->n_items <= 0) return 0;
-  return 2 * negf::gamma_stack_bytes(*p);
+  return 2 * negf::gamma_stack_bytes(*p) + negf::gamma_part_bytes(*p);
 }
 
 int negf_gamma_sum_run(const NegfGammaSum* p, void* stream) {
@@ -274,8 +303,18 @@ int negf_gamma_sum_run(const NegfGammaSum* p, void* stream) {
   const int sms = negf::sm_count_or(148);
   const int grid1 = p->n_items < sms ? p->n_items : sms;
   negf::gamma_stack_kernel<<<grid1, negf::CTA_THREADS, smem, s>>>(*p, Tst, Gst);
+  double* part = reinterpret_cast<double*>(reinterpret_cast<char*>(p->scratch) + 2 * negf::gamma_stack_bytes(*p));
   const int tiles = (p->n + negf::GT_M - 1) / negf::GT_M;
-  negf::gamma_reduce_kernel<<<dim3(tiles, tiles), negf::CTA_THREADS, smem, s>>>(*p, Tst, Gst);
+  const int64_t K = (int64_t)p->n_items * p->k;
+  int split = (2 * sms + tiles * tiles - 1) / (tiles * tiles);  // about two CTAs per SM
+  if (split > negf::GS_MAX_SPLIT) split = negf::GS_MAX_SPLIT;
+  if ((int64_t)split > (K + 255) / 256) split = (int)((K + 255) / 256);  // keep ranges >= 256 deep
+  if (split < 1) split = 1;
+  const int64_t klen = negf::gamma_split_len(K, split);
+  negf::gamma_reduce_kernel<<<dim3(tiles, tiles, split), negf::CTA_THREADS, smem, s>>>(*p, Tst, Gst, part, klen);
+  const int64_t n2 = (int64_t)p->n * p->n;
+  const int rgrid = (int)((n2 + 255) / 256 < 1024 ? (n2 + 255) / 256 : 1024);
+  negf::gamma_sum_parts_kernel<<<rgrid, 256, 0, s>>>(p->out, part, n2, split);
   return cudaGetLastError() == cudaSuccess ? NEGF_OK : NEGF_ERR_CUDA;
 }
 

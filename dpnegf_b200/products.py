@@ -114,13 +114,14 @@ def coupling_sigma(g: torch.Tensor, hdl: torch.Tensor, sdl: torch.Tensor, energi
 
 
 def lead_adjoint(hL, hLL, sL, sLL, hDL, sDL, E, eta, gs, gsig, form, tol=LEADADJ_TOL, max_iter=LEADADJ_MAX_ITER,
-                 stream=None):
+                 stream=None, info=None):
     """dL/d(hL, hLL, sL, sLL, hDL, sDL) through Sigma(E) of one lead (PyTorch's complex convention).
 
     ``E`` [B] complex (energy + E_ref), ``gs`` [B, n, n] the converged surface Green's functions at
     E + i eta, ``gsig`` [B, nc, nc] (form 0) or [B, n, n] (forms 1, 2) the incoming gradient of
     Sigma.  form 0: Sigma = (E S_DL - H_DL) g[:b,:b] (E S_DL^H - H_DL^H); 1: Sigma = g^-1;
-    2: Sigma = E S - H - g^-1.  Returns six tensors (None for hDL/sDL when not given)."""
+    2: Sigma = E S - H - g^-1.  Returns six tensors (None for hDL/sDL when not given); a dict
+    passed as ``info`` receives the doubling steps per energy under "iters"."""
     _lib.require_cuda()
     lib = _lib.load()
     dev = gs.device
@@ -154,16 +155,19 @@ def lead_adjoint(hL, hLL, sL, sLL, hDL, sDL, E, eta, gs, gsig, form, tol=LEADADJ
     items_t = _u8(items, dev)
     grad = torch.empty(4 * n * n + 2 * nc * b, dtype=C128, device=dev)
     status = torch.empty(B, dtype=torch.int32, device=dev)
+    iters = torch.empty(B, dtype=torch.int32, device=dev)
     p = _lib.NegfLeadAdjProblem()
     p.lead, p.arena, p.items, p.n_items, p.form = lead, arena.data_ptr(), items_t.data_ptr(), B, int(form)
     p.eta, p.tol, p.max_iter = float(eta), float(tol), int(max_iter)
     p.n_slots = max(1, min(B, lib.negf_sm_count()))
-    p.grad, p.status = grad.data_ptr(), status.data_ptr()
+    p.grad, p.status, p.iters = grad.data_ptr(), status.data_ptr(), iters.data_ptr()
     need = lib.negf_lead_adjoint_scratch_bytes(ctypes.byref(p))
     scratch = torch.empty(max(need, 256), dtype=torch.uint8, device=dev)
     p.scratch, p.scratch_bytes = scratch.data_ptr(), scratch.numel()
     _lib.check(lib.negf_lead_adjoint_run(ctypes.byref(p), _lib.stream_handle(stream)), "negf_lead_adjoint_run")
     st = status.cpu().numpy()
+    if info is not None:
+        info["iters"] = iters.cpu().numpy()
     if (st == _lib.NEGF_ERR_SINGULAR).any():
         raise torch.linalg.LinAlgError("lead adjoint: singular g_s or (zS - H - tau g_s tau')")
     if (st != _lib.NEGF_OK).any():

@@ -66,3 +66,52 @@ def test_run_rejects_bad_arguments_without_launch():
     lib = _lib.load()
     p = _lib.NegfRgfProblem()
     assert lib.negf_rgf_run(ctypes.byref(p), None) == _lib.NEGF_ERR_ARGUMENT
+
+
+def test_gamma_sum_rejects_bad_descriptors_without_launch():
+    """negf_gamma_sum_run validates its descriptor before any device call."""
+    lib = _lib.load()
+    p = _lib.NegfGammaSum()
+    assert lib.negf_gamma_sum_run(ctypes.byref(p), None) == _lib.NEGF_ERR_ARGUMENT
+    fake = 1 << 20  # never dereferenced: every case below fails a host-side check first
+    p.g = p.gamma = p.w = p.out = fake
+    p.n_items, p.n, p.c0, p.k, p.ldg, p.ldgam = 4, 32, 20, 16, 32, 16
+    assert lib.negf_gamma_sum_run(ctypes.byref(p), None) == _lib.NEGF_ERR_ARGUMENT  # c0 + k > ldg
+    p.c0 = 16
+    p.ldgam = 8
+    assert lib.negf_gamma_sum_run(ctypes.byref(p), None) == _lib.NEGF_ERR_ARGUMENT  # ldgam < k
+    p.ldgam = 16
+    need = lib.negf_gamma_sum_scratch_bytes(ctypes.byref(p))
+    assert need >= 2 * 32 * 4 * 16 * 16 and need % 256 == 0
+    p.scratch, p.scratch_bytes = fake, need - 1
+    assert lib.negf_gamma_sum_run(ctypes.byref(p), None) == _lib.NEGF_ERR_ARGUMENT  # scratch too small
+    p.scratch_bytes, p.g = need, fake + 8
+    assert lib.negf_gamma_sum_run(ctypes.byref(p), None) == _lib.NEGF_ERR_ARGUMENT  # G not 16-byte aligned
+    p.g, p.n_items, p.k, p.ldg, p.ldgam = fake, 1 << 24, 512, 1024, 512
+    assert lib.negf_gamma_sum_run(ctypes.byref(p), None) == _lib.NEGF_ERR_UNSUPPORTED  # n_items k > 2^31
+
+
+def test_lead_adjoint_rejects_bad_descriptors_without_launch():
+    """negf_lead_adjoint_run validates its descriptor before any device call."""
+    lib = _lib.load()
+    p = _lib.NegfLeadAdjProblem()
+    assert lib.negf_lead_adjoint_run(ctypes.byref(p), None) == _lib.NEGF_ERR_ARGUMENT
+    fake = 1 << 20
+    p.arena = p.items = p.grad = p.status = p.scratch = fake
+    p.lead.n, p.lead.nc, p.lead.b, p.lead.hdl, p.lead.sdl = 24, 10, 8, 0, 80
+    p.n_items, p.n_slots, p.max_iter = 6, 2, 64
+    p.form = 3
+    assert lib.negf_lead_adjoint_run(ctypes.byref(p), None) == _lib.NEGF_ERR_ARGUMENT  # unknown form
+    p.form = 0
+    p.lead.nc = 0
+    assert lib.negf_lead_adjoint_run(ctypes.byref(p), None) == _lib.NEGF_ERR_ARGUMENT  # coupling form, no H_DL
+    p.lead.nc, p.lead.b = 10, 30
+    assert lib.negf_lead_adjoint_run(ctypes.byref(p), None) == _lib.NEGF_ERR_ARGUMENT  # b > n
+    p.lead.b = 8
+    need = lib.negf_lead_adjoint_scratch_bytes(ctypes.byref(p))
+    assert need == 2 * ((18 * 24 * 24 + 15) // 16 * 16) * 16
+    p.scratch_bytes = need - 16
+    assert lib.negf_lead_adjoint_run(ctypes.byref(p), None) == _lib.NEGF_ERR_ARGUMENT  # scratch too small
+    p.lead.n = 600
+    p.scratch_bytes = lib.negf_lead_adjoint_scratch_bytes(ctypes.byref(p))
+    assert lib.negf_lead_adjoint_run(ctypes.byref(p), None) == _lib.NEGF_ERR_UNSUPPORTED  # n > NEGF_MAX_BLOCK

@@ -24,7 +24,14 @@ constexpr int PITCH_MK = GT_K + 4;  // [64 rows][GT_K k] tiles (pitch = 4 mod 8)
 constexpr int PITCH_KN = GT_N + 2;  // [GT_K k][64 cols] tiles (pitch = 2 mod 8)
 constexpr int GT_LOADS = GT_M * GT_K / 256;  // 16-byte copies per thread per operand tile
 constexpr int GT_TILE = (GT_M * PITCH_MK > GT_K * PITCH_KN) ? GT_M * PITCH_MK : GT_K * PITCH_KN;
-constexpr int GT_STAGES = 3;
+#ifndef NEGF_GT_STAGES
+#define NEGF_GT_STAGES 3
+#endif
+// Depth of the cp.async k-slab ring; one value for the whole library (the host-side shared-memory
+// sizes of every kernel derive from it).  4 stages measured 4 % slower on the 256^3 product and
+// the sweep (LU solves 2 % faster).
+constexpr int GT_STAGES = NEGF_GT_STAGES;
+static_assert(GT_STAGES == 3 || GT_STAGES == 4, "3- or 4-stage ring");
 constexpr int GEMM_SMEM_BYTES = 2 * GT_STAGES * GT_TILE * (int)sizeof(cplx);  // stages x (A,B)
 constexpr int CTA_THREADS = 256;
 

@@ -144,12 +144,29 @@ NEGF_DEV void ls_item(const NegfLsProblem& P, const NegfLsItem& it, cplx* slot, 
       epss[e] = cadd(epss[e], bXa);
       AB2[e] = aXa;
       AB2[n2 + e] = bXb;
-      const double v = hypot(aXa.x, aXa.y) + hypot(bXb.x, bXb.y);
+      const double v = cabs1(aXa) + cabs1(bXb);  // bounds |aXa| + |bXb| within a factor sqrt(2)
       m = (v == v) ? fmax(m, v) : INFINITY;
     }
     cplx* t = AB; AB = AB2; AB2 = t;
     m = cta_max(m, red);  // begins with a barrier: the pass above is complete
-    if (m < P.tol) { converged = true; break; }
+    // The reference's test is max(|alpha| + |beta|) < tol with complex moduli.  Since
+    // cabs1(z) / sqrt(2) <= |z| <= cabs1(z), the bound m decides it (with 8 ulp of slack for the
+    // rounding of both sums) unless m lies within a factor sqrt(2) of tol; only then are the
+    // moduli summed, so the decision and the step count are those of the moduli.
+    constexpr double SLACK = 8.0 * 2.220446049250313e-16, RSQRT2 = 0.70710678118654752440;
+    bool conv = false;
+    if (isfinite(m) && m * (1.0 + SLACK) < P.tol) {
+      conv = true;
+    } else if (isfinite(m) && m * (1.0 - SLACK) * RSQRT2 < P.tol) {
+      double x = 0.0;
+      for (int e = threadIdx.x; e < n2; e += CTA_THREADS) {
+        const double v = hypot(AB[e].x, AB[e].y) + hypot(AB[n2 + e].x, AB[n2 + e].y);
+        x = (v == v) ? fmax(x, v) : INFINITY;
+      }
+      m = cta_max(x, red);
+      conv = m < P.tol;
+    }
+    if (conv) { converged = true; break; }
     if (!isfinite(m)) break;
   }
 

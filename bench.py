@@ -56,11 +56,14 @@ def parse():
     ap.add_argument("--configs", default="",
                     help="extra legs, comma separated: 'uneven' (the 512-device uneven batch, 128 devices), "
                          "'leads' (its lead decimation alone, --lead-devices devices), 'scf' (b=512 SCF "
-                         "loop captured as a CUDA graph) and 'products' (the G Gamma G^H sum, the Bloch "
-                         "coupling product and the lead adjoint, each timed alone); not in the default run")
+                         "loop captured as a CUDA graph), not in the default run; 'products' (the G Gamma "
+                         "G^H sum, the Bloch coupling product and the lead adjoint, each timed alone) is in "
+                         "the default line unless --no-products")
     ap.add_argument("--lead-devices", type=int, default=128, help="devices whose leads the 'leads' leg decimates")
     ap.add_argument("--lead-eta", type=float, default=1e-5, help="lead broadening of the 'leads' leg")
     ap.add_argument("--no-leads", action="store_true", help="skip the metric device's lead decimation object")
+    ap.add_argument("--no-products", action="store_true",
+                    help="skip the product-chain timings (G Gamma G^H sum, Bloch coupling, lead adjoint)")
     ap.add_argument("--uneven-devices", type=int, default=128, help="devices of the 'uneven' leg")
     ap.add_argument("--uneven-chunk", type=int, default=128, help="devices per launch in the 'uneven' leg")
     ap.add_argument("--scf-k", type=int, default=8, help="k-points of the 'scf' leg")
@@ -911,8 +914,9 @@ def main():
         if "scf" in wanted:
             extra["config5_scf"] = scf_leg(torch, peak, nk=args.scf_k, n_energies=args.scf_energies,
                                            iters=args.scf_iters, eta_lead=args.lead_eta)
-        if "products" in wanted:
-            extra["product_chains"] = products_leg(torch, peak, eta=args.lead_eta)
+    # the product chains (default line, or asked for with --configs products)
+    if rank == 0 and (not args.no_products or "products" in args.configs.split(",")):
+        extra["product_chains"] = products_leg(torch, peak, eta=args.lead_eta)
 
     # end-to-end through the public API: pinned host inputs, host outputs
     e2e = None

@@ -220,6 +220,25 @@ def require_cuda():
     load()
 
 
+def on_given_stream(fn):
+    """Run ``fn`` with its ``stream`` keyword as torch's current stream.
+
+    The wrappers stage descriptor tables and scratch in torch tensors, launch, and may read a
+    status back; with the caller's stream current for the whole call, all of that is ordered on
+    that one stream, so the caching allocator hands the staging memory to other work only behind
+    the launch, and host reads see the kernel's writes.  Results belong to that stream."""
+    import functools
+
+    @functools.wraps(fn)
+    def wrapped(*args, stream=None, **kw):
+        if stream is None:
+            return fn(*args, stream=None, **kw)
+        import torch
+        with torch.cuda.stream(stream):
+            return fn(*args, stream=None, **kw)
+    return wrapped
+
+
 def stream_handle(torch_stream=None):
     import torch
     s = torch_stream if torch_stream is not None else torch.cuda.current_stream()

@@ -34,6 +34,7 @@ def _rows_contiguous(t):
     return t if t.stride(-1) == 1 else t.contiguous()
 
 
+@_lib.on_given_stream
 def gamma_sum(G: torch.Tensor, gamma: torch.Tensor, c0: int, w: torch.Tensor, stream=None) -> torch.Tensor:
     """sum_i w_i Re(G_i[:, c0:c0+k] gamma_i G_i[:, c0:c0+k]^H) as a real [n, n] tensor.
 
@@ -66,6 +67,7 @@ def gamma_sum(G: torch.Tensor, gamma: torch.Tensor, c0: int, w: torch.Tensor, st
     return out
 
 
+@_lib.on_given_stream
 def coupling_sigma(g: torch.Tensor, hdl: torch.Tensor, sdl: torch.Tensor, energies, E_ref=0.0,
                    stream=None) -> torch.Tensor:
     """Sigma_i = (E_i S_DL - H_DL) g_i[:b,:b] (E_i S_DL^H - H_DL^H), E_i = energies_i + E_ref.
@@ -113,6 +115,7 @@ def coupling_sigma(g: torch.Tensor, hdl: torch.Tensor, sdl: torch.Tensor, energi
     return sig
 
 
+@_lib.on_given_stream
 def lead_adjoint(hL, hLL, sL, sLL, hDL, sDL, E, eta, gs, gsig, form, tol=LEADADJ_TOL, max_iter=LEADADJ_MAX_ITER,
                  stream=None, info=None):
     """dL/d(hL, hLL, sL, sLL, hDL, sDL) through Sigma(E) of one lead (PyTorch's complex convention).

@@ -203,6 +203,7 @@ _FAMILY = {  # output tag -> (flag, block field, shape fn (n_q, n_next, n_last))
 }
 
 
+@_lib.on_given_stream
 def run(geom: Geometry, energies: List[torch.Tensor], se_l: List[Optional[torch.Tensor]],
         se_r: List[Optional[torch.Tensor]], eta=0.0, E_ref=0.0, outputs=("g_trans", "grd", "grl", "gru"),
         trans=False, orb_dos=False, dos=False, orb_g=False, orb_ar=False,

@@ -98,6 +98,7 @@ class LeadArena:
         self.table = np.array(table, dtype=_lib.LEAD_DTYPE)
 
 
+@_lib.on_given_stream
 def self_energies(arena: LeadArena, lead_index: Sequence[int], energies, eta, E_ref=0.0, want_gs=False,
                   want_sigma=True, tol=LS_TOL, max_iter=LS_MAX_ITER, check=True, n_slots=None, stream=None):
     """Decimate every (lead_index[i], energies[i]) pair in one launch.

@@ -145,3 +145,41 @@ def test_lead_adjoint_without_s_dl():
     assert got[5] is None and ref[5] is None
     for x, y in zip(got[:5], ref[:5]):
         assert _rel(x, y) < 1e-10
+
+
+def test_wrappers_on_a_side_stream_match_the_current_stream():
+    """Called with a side stream, the wrappers stage, launch and read back on that stream: results
+    equal the current-stream call bit for bit."""
+    from dpnegf_b200 import surface_green as sg
+    from dpnegf_b200.products import coupling_sigma, gamma_sum, lead_adjoint
+    gen = torch.Generator().manual_seed(21)
+    G, gam, w = _rand((9, 40, 40), gen).cuda(), _rand((9, 12, 12), gen).cuda(), torch.rand(9, dtype=torch.float64)
+    hL, hLL, sL, sLL = _lead_blocks(16, gen)
+    hDL = _rand((10, 16), gen, 0.4).cuda()
+    E = np.linspace(-0.8, 0.8, 5)
+    arena = sg.LeadArena([sg.LeadBlocks(hL, hLL, sL, sLL, hDL, None)], device="cuda")
+    gsig = _rand((5, 10, 10), gen).cuda()
+
+    def run(stream):
+        def inputs_ready():  # the glue below runs on the current stream
+            if stream is not None:
+                stream.wait_stream(torch.cuda.current_stream())
+        inputs_ready()
+        out = [gamma_sum(G, gam, 28, w, stream=stream)]
+        inputs_ready()
+        res = sg.self_energies(arena, [0] * 5, E, 1e-3, want_gs=True, stream=stream)
+        gs = torch.stack(res.gs)
+        out += [gs, torch.stack(res.sigma)]
+        inputs_ready()
+        out.append(coupling_sigma(gs, hDL, None, E, stream=stream))
+        inputs_ready()
+        out += [x for x in lead_adjoint(hL, hLL, sL, sLL, hDL, None, E, 1e-3, gs, gsig, 0, stream=stream)
+                if x is not None]
+        return out
+
+    ref = run(None)
+    side = torch.cuda.Stream()
+    got = run(side)
+    side.synchronize()
+    for x, y in zip(got, ref):
+        assert torch.equal(x, y)

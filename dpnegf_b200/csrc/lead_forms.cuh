@@ -43,18 +43,19 @@ NEGF_DEV double cta_max(double v, double* red) {
   return m;
 }
 
-// C = alpha op(A) op(B) (+ beta D when D is given).  Conventional 4M complex products (see
-// warp_mma_3m): the lead iterations square and accumulate products, which amplifies the looser
-// componentwise error of Gauss/3M products.  Lead blocks come in every size, so warps outside
-// the product skip their MMAs.
-template <int OPA, int OPB>
+// C = alpha op(A) op(B) (+ beta D when D is given).  By default conventional 4M complex products
+// (see warp_mma_3m): the decimation squares and accumulates products, which amplifies the looser
+// componentwise error of Gauss/3M products; G3 = true selects Gauss/3M where no iteration feeds
+// rounding back into the result.  Lead blocks come in every size, so warps outside the product
+// skip their MMAs.
+template <int OPA, int OPB, bool G3 = false>
 NEGF_DEV void gemm_ls(cplx* smem, int M, int N, int K, const cplx* A, int64_t lda, const cplx* B, int64_t ldb,
                       cplx* C, int64_t ldc, const cplx* D = nullptr, int64_t ldd = 0,
                       cplx alpha = cmk(1.0, 0.0), cplx beta = cmk(1.0, 0.0)) {
   GemmArgs g = gemm_args(M, N, K, A, lda, B, ldb, C, ldc);
   g.alpha = alpha;
   if (D) { g.D = D; g.ldd = ldd; g.beta = beta; g.use_d = true; }
-  cta_gemm<OPA, OPB, false, true>(g, smem);
+  cta_gemm<OPA, OPB, G3, true>(g, smem);
 }
 
 // out = W^-1 (n x n, row stride n) by the LU solve against I (numpy.linalg.inv's route); W is

@@ -8,8 +8,9 @@
 //                           g_s = (zS - H - tau g_s tau')^-1, the relation the reference's residual
 //                           check tests, negf/surface_green.py:142-145)
 //
-// Both are batched over energies and use the CTA tile GEMM of the sweep (DMMA, 4M complex
-// products) and the pivoted LU of the decimation.  Sums over energies run in a fixed order, so
+// Both are batched over energies and use the CTA tile GEMM of the sweep (DMMA, Gauss/3M complex
+// products, as the sweep: no iteration here feeds rounding back) and the pivoted LU of the
+// decimation.  Sums over energies run in a fixed order, so
 // results are bitwise reproducible.
 #include "../../include/negf_b200.h"
 #include "lead_forms.cuh"
@@ -48,7 +49,7 @@ __global__ void __launch_bounds__(CTA_THREADS, 1) gamma_stack_kernel(const NegfG
   for (int i = blockIdx.x; i < P.n_items; i += gridDim.x) {
     const cplx* G = reinterpret_cast<const cplx*>(P.g) + (int64_t)i * P.g_stride + P.c0;
     const cplx* Gam = reinterpret_cast<const cplx*>(P.gamma) + (int64_t)i * P.gamma_stride;
-    gemm_ls<OP_N, OP_N>(smem, P.n, P.k, P.k, G, P.ldg, Gam, P.ldgam, Tst + (int64_t)i * P.k, K, nullptr, 0,
+    gemm_ls<OP_N, OP_N, true>(smem, P.n, P.k, P.k, G, P.ldg, Gam, P.ldgam, Tst + (int64_t)i * P.k, K, nullptr, 0,
                         cmk(P.w[i], 0.0));
     for (int64_t e = threadIdx.x; e < (int64_t)P.n * P.k; e += CTA_THREADS) {
       const int64_t r = e / P.k, c = e % P.k;
@@ -82,7 +83,7 @@ __global__ void __launch_bounds__(CTA_THREADS, 1) gamma_reduce_kernel(const Negf
     return;
   }
   GemmArgs g = gemm_args(M, N, Kz, Tst + (int64_t)m0 * K + k0, K, Gst + (int64_t)n0 * K + k0, K, nullptr, 0);
-  cta_gemm_epi<OP_N, OP_C, false, EpiRealOut, true>(g, smem, EpiRealOut{out, P.n, m0, n0});
+  cta_gemm_epi<OP_N, OP_C, true, EpiRealOut, true>(g, smem, EpiRealOut{out, P.n, m0, n0});
 }
 
 // Stage 3: out = sum of the partial outputs in range order.
@@ -155,11 +156,11 @@ NEGF_DEV void la_item(const NegfLeadAdjProblem& P, int idx, cplx* slot, char* sm
     for (int e = threadIdx.x; e < nc * b; e += CTA_THREADS) Lm[e] = csub(cmul(E, sdl[e]), hdl[e]);
     __syncthreads();
     form_eS_minus_h_herm(Rm, hdl, sdl, E, b, nc);                       // b x nc
-    gemm_ls<OP_C, OP_N>(smem, b, nc, nc, Lm, b, Gs, nc, T1, nc);        // L^H Gs       (b x nc)
-    gemm_ls<OP_N, OP_C>(smem, b, b, nc, T1, nc, Rm, nc, lam, n);        // V[:b,:b]
-    gemm_ls<OP_N, OP_C>(smem, nc, b, nc, Gs, nc, Rm, nc, T2, b);        // Gs R^H       (nc x b)
-    gemm_ls<OP_N, OP_C>(smem, nc, b, b, T2, b, g, n, gL, b);            // dL/dL        (nc x b)
-    gemm_ls<OP_C, OP_N>(smem, b, nc, b, g, n, T1, nc, gR, nc);          // dL/dR        (b x nc)
+    gemm_ls<OP_C, OP_N, true>(smem, b, nc, nc, Lm, b, Gs, nc, T1, nc);        // L^H Gs       (b x nc)
+    gemm_ls<OP_N, OP_C, true>(smem, b, b, nc, T1, nc, Rm, nc, lam, n);        // V[:b,:b]
+    gemm_ls<OP_N, OP_C, true>(smem, nc, b, nc, Gs, nc, Rm, nc, T2, b);        // Gs R^H       (nc x b)
+    gemm_ls<OP_N, OP_C, true>(smem, nc, b, b, T2, b, g, n, gL, b);            // dL/dL        (nc x b)
+    gemm_ls<OP_C, OP_N, true>(smem, b, nc, b, g, n, T1, nc, gR, nc);          // dL/dR        (b x nc)
     const cplx Ec = cconj(E);
     for (int e = threadIdx.x; e < nc * b; e += CTA_THREADS) {
       const int i = e / b, j = e % b;
@@ -172,8 +173,8 @@ NEGF_DEV void la_item(const NegfLeadAdjProblem& P, int idx, cplx* slot, char* sm
     for (int64_t e = threadIdx.x; e < n2; e += CTA_THREADS) F[e] = g[e];
     __syncthreads();
     bad |= cta_lu_inverse(F, W, n, smem_raw);                           // W = g^-1
-    gemm_ls<OP_C, OP_N>(smem, n, n, n, W, n, Gs, n, T1, n);             // g^-H Gs
-    gemm_ls<OP_N, OP_C>(smem, n, n, n, T1, n, W, n, lam, n, nullptr, 0, P.form == 1 ? MONE : ONE);
+    gemm_ls<OP_C, OP_N, true>(smem, n, n, n, W, n, Gs, n, T1, n);             // g^-H Gs
+    gemm_ls<OP_N, OP_C, true>(smem, n, n, n, T1, n, W, n, lam, n, nullptr, 0, P.form == 1 ? MONE : ONE);
     if (P.form == 2) {
       const cplx Ec = cconj(E);
       for (int64_t e = threadIdx.x; e < n2; e += CTA_THREADS) {
@@ -187,16 +188,16 @@ NEGF_DEV void la_item(const NegfLeadAdjProblem& P, int idx, cplx* slot, char* sm
   // ---- Lambda by doubling
   cta_shift_form(tau, H01, S01, z, MONE, (int)n2, smem);                // z S01 - H01
   form_eS_minus_h_herm(taup, H01, S01, z, n, n);                        // z S01^H - H01^H
-  gemm_ls<OP_N, OP_N>(smem, n, n, n, g, n, tau, n, Pm, n);              // P = g tau
-  gemm_ls<OP_N, OP_N>(smem, n, n, n, taup, n, g, n, Qm, n);             // Q = tau' g
+  gemm_ls<OP_N, OP_N, true>(smem, n, n, n, g, n, tau, n, Pm, n);              // P = g tau
+  gemm_ls<OP_N, OP_N, true>(smem, n, n, n, taup, n, g, n, Qm, n);             // Q = tau' g
   int steps = 0;
   bool finite = true;
   for (int s = 0; s < P.max_iter; ++s) {
     steps = s + 1;
-    gemm_ls<OP_C, OP_N>(smem, n, n, n, Pm, n, lam, n, T1, n);           // P^H Lambda
-    gemm_ls<OP_N, OP_C>(smem, n, n, n, T1, n, Qm, n, lam, n, lam, n);   // Lambda += ... Q^H
-    gemm_ls<OP_N, OP_N>(smem, n, n, n, Pm, n, Pm, n, P2, n);
-    gemm_ls<OP_N, OP_N>(smem, n, n, n, Qm, n, Qm, n, Q2, n);
+    gemm_ls<OP_C, OP_N, true>(smem, n, n, n, Pm, n, lam, n, T1, n);           // P^H Lambda
+    gemm_ls<OP_N, OP_C, true>(smem, n, n, n, T1, n, Qm, n, lam, n, lam, n);   // Lambda += ... Q^H
+    gemm_ls<OP_N, OP_N, true>(smem, n, n, n, Pm, n, Pm, n, P2, n);
+    gemm_ls<OP_N, OP_N, true>(smem, n, n, n, Qm, n, Qm, n, Q2, n);
     cplx* t = Pm; Pm = P2; P2 = t;
     t = Qm; Qm = Q2; Q2 = t;
     double mp = 0.0, mq = 0.0;
@@ -212,16 +213,16 @@ NEGF_DEV void la_item(const NegfLeadAdjProblem& P, int idx, cplx* slot, char* sm
   }
 
   // ---- F = (zS - H - tau g tau')^-1 and the parameter gradients
-  gemm_ls<OP_N, OP_N>(smem, n, n, n, g, n, taup, n, Y1, n);             // g tau'
-  gemm_ls<OP_N, OP_N>(smem, n, n, n, tau, n, Y1, n, W, n);              // tau g tau'
+  gemm_ls<OP_N, OP_N, true>(smem, n, n, n, g, n, taup, n, Y1, n);             // g tau'
+  gemm_ls<OP_N, OP_N, true>(smem, n, n, n, tau, n, Y1, n, W, n);              // tau g tau'
   for (int64_t e = threadIdx.x; e < n2; e += CTA_THREADS) W[e] = csub(csub(cmul(z, S[e]), H[e]), W[e]);
   __syncthreads();
   bad |= cta_lu_inverse(W, F, n, smem_raw);
-  gemm_ls<OP_C, OP_N>(smem, n, n, n, F, n, lam, n, T1, n);              // F^H Lambda
-  gemm_ls<OP_N, OP_C>(smem, n, n, n, T1, n, F, n, gW, n, nullptr, 0, MONE);  // dW
-  gemm_ls<OP_N, OP_C>(smem, n, n, n, gW, n, Y1, n, T1, n, nullptr, 0, MONE);  // dtau = -dW (g tau')^H
-  gemm_ls<OP_N, OP_N>(smem, n, n, n, tau, n, g, n, Pm, n);              // tau g
-  gemm_ls<OP_C, OP_N>(smem, n, n, n, Pm, n, gW, n, Qm, n, nullptr, 0, MONE);  // dtau' = -(tau g)^H dW
+  gemm_ls<OP_C, OP_N, true>(smem, n, n, n, F, n, lam, n, T1, n);              // F^H Lambda
+  gemm_ls<OP_N, OP_C, true>(smem, n, n, n, T1, n, F, n, gW, n, nullptr, 0, MONE);  // dW
+  gemm_ls<OP_N, OP_C, true>(smem, n, n, n, gW, n, Y1, n, T1, n, nullptr, 0, MONE);  // dtau = -dW (g tau')^H
+  gemm_ls<OP_N, OP_N, true>(smem, n, n, n, tau, n, g, n, Pm, n);              // tau g
+  gemm_ls<OP_C, OP_N, true>(smem, n, n, n, Pm, n, gW, n, Qm, n, nullptr, 0, MONE);  // dtau' = -(tau g)^H dW
   const cplx zc = cconj(z);
   for (int64_t e = threadIdx.x; e < n2; e += CTA_THREADS) {
     const int64_t i = e / n, j = e % n;

@@ -52,33 +52,4 @@ NEGF_DEV void cta_shift_form(cplx* out, const cplx* X, const cplx* Y, cplx z, cp
   __syncthreads();
 }
 
-// out = alpha * (X - z Y)^T: X, Y are m x n (row stride n), out is n x m (row stride m); a null
-// Y is zero.  Through 32 x 32 shared-memory tiles so reads and writes are both coalesced.
-// out must not alias X or Y.  Ends with __syncthreads().
-NEGF_DEV void cta_transpose_shift(cplx* out, const cplx* X, const cplx* Y, cplx z, cplx alpha, int m, int n,
-                                  cplx* smem) {
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
-  cplx* tile = smem;                                       // [32][33]
-  for (int i0 = 0; i0 < m; i0 += 32)
-    for (int j0 = 0; j0 < n; j0 += 32) {
-#pragma unroll
-      for (int r = ty; r < 32; r += 8) {
-        const int i = i0 + r, j = j0 + tx;
-        cplx v = cmk(0.0, 0.0);
-        if (i < m && j < n) {
-          const int64_t e = (int64_t)i * n + j;
-          v = Y ? csub(X[e], cmul(z, Y[e])) : X[e];
-        }
-        tile[r * 33 + tx] = cmul(alpha, v);
-      }
-      __syncthreads();
-#pragma unroll
-      for (int r = ty; r < 32; r += 8) {
-        const int j = j0 + r, i = i0 + tx;
-        if (i < m && j < n) out[(int64_t)j * m + i] = tile[tx * 33 + r];
-      }
-      __syncthreads();
-    }
-}
-
 }  // namespace negf

@@ -502,9 +502,10 @@ NEGF_DEV void rgf_item(const NegfRgfProblem& P, const NegfItem& it, const SlotBu
   const int ck = (adj && P.ckpt > 0) ? P.ckpt : 0;
   const int nck = ck ? (K + ck - 1) / ck : 0;
   const size_t mn2 = (size_t)P.max_n * P.max_n;
+  const int ckd = ck ? ck : 1;  // divisor for the checkpoint layout (unused when ck == 0)
   auto slab_ptr = [&](cplx* slab, int q) -> cplx* {
     if (!ck) return slab + blk[q].g;
-    return slab + (size_t)(q % ck == 0 ? q / ck : nck + q % ck) * mn2;
+    return slab + (size_t)(q % ckd == 0 ? q / ckd : nck + q % ckd) * mn2;
   };
   auto gptr = [&](int q) -> cplx* {
     return (fl & NEGF_OUT_GR_LEFT) ? out + blk[q].o_grleft + row * sq(q) : slab_ptr(sb.gslab, q);

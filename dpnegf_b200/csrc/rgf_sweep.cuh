@@ -268,7 +268,7 @@ __device__ __noinline__ int cta_inverse_blk(cplx* W, int64_t ldw, int n, cplx* G
 // sign vector v (entries +-1 +-i from a hash of the index), y = G v and
 // r = A y - v; true when max|r| <= tol n max|A| max|y| (a backward-stable
 // inverse leaves about n u there) and everything is finite.  Whole CTA (the
-// verdict is uniform); y lives in smem.
+// decision is uniform); y lives in smem.
 NEGF_DEV bool inv_probe(const cplx* A, const cplx* G, int n, double tol, cplx* smem, double* red) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   auto v = [](int j) {

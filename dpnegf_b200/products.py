@@ -40,8 +40,6 @@ def gamma_sum(G: torch.Tensor, gamma: torch.Tensor, c0: int, w: torch.Tensor, st
 
     ``G`` [B, n, m] and ``gamma`` [B, k, k] complex128 CUDA tensors (views allowed when their rows
     are contiguous), ``w`` [B] real weights.  Bitwise reproducible (fixed summation order)."""
-    _lib.require_cuda()
-    lib = _lib.load()
     if G.ndim != 3 or gamma.ndim != 3 or G.shape[0] != gamma.shape[0]:
         raise ValueError("G [B, n, m] and gamma [B, k, k] with the same B")
     B, n, m = G.shape
@@ -54,6 +52,8 @@ def gamma_sum(G: torch.Tensor, gamma: torch.Tensor, c0: int, w: torch.Tensor, st
     w = torch.as_tensor(w, dtype=torch.float64).reshape(-1).to(dev).contiguous()
     if w.shape[0] != B:
         raise ValueError(f"{w.shape[0]} weights for {B} energies")
+    _lib.require_cuda()
+    lib = _lib.load()
     out = torch.empty(n, n, dtype=torch.float64, device=dev)
     p = _lib.NegfGammaSum()
     p.g, p.g_stride, p.ldg = G.data_ptr(), G.stride(0), G.stride(1)
@@ -74,8 +74,6 @@ def coupling_sigma(g: torch.Tensor, hdl: torch.Tensor, sdl: torch.Tensor, energi
 
     ``g`` [B, N, N] complex128 CUDA tensor, ``hdl``/``sdl`` [nc, b] (b <= N; ``sdl`` may be None).
     One launch of the decimation kernel in its coupling-product mode; returns [B, nc, nc]."""
-    _lib.require_cuda()
-    lib = _lib.load()
     dev = g.device
     g = g.to(C128).resolve_conj().contiguous()
     B, N = g.shape[0], g.shape[-1]
@@ -87,6 +85,8 @@ def coupling_sigma(g: torch.Tensor, hdl: torch.Tensor, sdl: torch.Tensor, energi
     E = np.asarray(energies, dtype=np.complex128).reshape(-1) + complex(E_ref)
     if E.shape[0] != B:
         raise ValueError(f"{E.shape[0]} energies for {B} surface Green's functions")
+    _lib.require_cuda()
+    lib = _lib.load()
     arena = torch.cat([hdl.reshape(-1), sdl.reshape(-1)])
     lead = np.zeros((), dtype=_lib.LEAD_DTYPE)
     lead["n"], lead["nc"], lead["b"] = N, nc, b
@@ -125,8 +125,10 @@ def lead_adjoint(hL, hLL, sL, sLL, hDL, sDL, E, eta, gs, gsig, form, tol=LEADADJ
     Sigma.  form 0: Sigma = (E S_DL - H_DL) g[:b,:b] (E S_DL^H - H_DL^H); 1: Sigma = g^-1;
     2: Sigma = E S - H - g^-1.  Returns six tensors (None for hDL/sDL when not given); a dict
     passed as ``info`` receives the doubling steps per energy under "iters"."""
-    _lib.require_cuda()
-    lib = _lib.load()
+    if form not in (0, 1, 2):
+        raise ValueError(f"form must be 0, 1 or 2, not {form!r}")
+    if form == 0 and hDL is None:
+        raise ValueError("form 0 (the coupling form) needs H_DL")
     dev = gs.device
     c = lambda t: torch.as_tensor(t).to(dev, C128).resolve_conj().contiguous()
     hL, hLL, sL, sLL = c(hL), c(hLL), c(sL), c(sLL)
@@ -149,8 +151,13 @@ def lead_adjoint(hL, hLL, sL, sLL, hDL, sDL, E, eta, gs, gsig, form, tol=LEADADJ
             raise ValueError(f"dL/dSigma {tuple(gsig.shape)} is not [B, {nc}, {nc}]")
     elif gsig.shape[-2:] != (n, n):
         raise ValueError(f"dL/dSigma {tuple(gsig.shape)} is not [B, {n}, {n}]")
-    arena = torch.cat(pieces)
     E = np.asarray(torch.as_tensor(E).detach().cpu().numpy(), dtype=np.complex128).reshape(-1)
+    if E.shape[0] != B or gs.shape[-2:] != (n, n) or gsig.ndim != 3 or gsig.shape[0] != B:
+        raise ValueError(f"{E.shape[0]} energies, g_s {tuple(gs.shape)} and dL/dSigma {tuple(gsig.shape)} "
+                         f"for a {n}-wide lead: one [n, n] g_s and one dL/dSigma per energy")
+    _lib.require_cuda()
+    lib = _lib.load()
+    arena = torch.cat(pieces)
     items = np.zeros(B, dtype=_lib.LEADADJ_ITEM_DTYPE)
     items["e_re"], items["e_im"] = E.real, E.imag
     items["gs"] = gs.data_ptr() + np.arange(B, dtype=np.uint64) * (n * n * 16)
